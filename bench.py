@@ -1,0 +1,361 @@
+"""Benchmark of the Zstd L2 batched match-find workload on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gcz|reference]
+
+Workload (one "step"): Zstd L2 match finding over a 1 GiB synthetic input
+(seed 2; 40% order-1 Markov / 40% copies with offsets log-uniform to 8 MiB /
+20% random; 16384 independent 64 KiB windows; search depth 64, which behaves
+exactly like depth 16) in one launch, producing the ZSTD_Sequence records
+ZSTD_compressSequences consumes.  Each rank processes its own 1 GiB shard
+(weak scaling, no collective on the data path).
+
+`value`: input GB/s (1e9 B/s) with the input already in HBM (device entry
+point), K steps timed with CUDA events on the launch stream; the input is
+larger than L2 (126 MB), so no flush is needed between steps.
+`e2e`: the same metric through the host-buffer C-ABI call
+(gcz_zstd_match_find) from pinned memory: H2D of the input, kernels, D2H of
+the sequences and per-window offsets, all inside the timed region.
+`--impl reference`: the reference's path timed on this box -- its CPU
+restatement (oracle port, all host threads) as `value`, plus the reference's
+own kernels (PTX compiled from its sources, JIT-loaded) on the same GPU.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-compressor_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "input GB/s per B200 (match-find, end-to-end)"
+WORKLOAD = "zstd_l2_batched_1gib"
+N_BYTES = 1 << 30
+SEED = 2
+DEPTH = 64
+HBM_FALLBACK = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gcz", choices=["gcz", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_mod
+
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+    else:
+        torch.cuda.set_device(local)
+    return world, rank, local, dist
+
+
+def barrier(dist, torch, local):
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(dist, torch, value):
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, torch, value):
+    if dist is None:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_oracle_time(data, depth, threads):
+    from oracle import oracle as orc
+
+    t0 = time.perf_counter()
+    seqs, off = orc.zstd_sequences(data, depth, threads=threads)
+    dt = time.perf_counter() - t0
+    return dt, int(off[-1])
+
+
+def run_gcz(args):
+    import torch
+    import gcz
+
+    world, rank, local, dist = dist_setup(args)
+    dev = torch.device("cuda", local)
+    ctx = gcz.Context(local)
+    n = N_BYTES
+    data = gcz.gen_synthetic(SEED + 1000 * rank, n, 8 << 20)
+    B = gcz.num_windows(n)
+    d_in = torch.from_numpy(data).to(dev)
+    cap = int(gcz.L.gcz_zstd_max_sequences(n))
+    d_seqs = torch.empty((cap, 4), dtype=torch.int32, device=dev)
+    d_off = torch.empty(B + 1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        ctx.zstd_match_find_device(d_in.data_ptr(), n, DEPTH, d_seqs.data_ptr(), cap, d_off.data_ptr(), sp)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.sync(sp)
+    nseq = int(d_off[-1].item())
+
+    # ---- device-resident timing
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, torch, local)
+    with Clocks(local) as clk:
+        ctx.profile_start()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        kern_ms, kern_launches, all_launches = ctx.profile_stop()
+    barrier(dist, torch, local)
+    ctx.sync(sp)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(dist, torch, ms)
+    value = world * n * args.steps / (ms_max / 1e3) / 1e9
+
+    # ---- end-to-end through the host-buffer C-ABI call (pinned buffers)
+    h_in = torch.from_numpy(data).pin_memory()
+    h_seqs = torch.empty((nseq + 1024, 4), dtype=torch.int32).pin_memory()
+    h_off = torch.empty(B + 1, dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        rc = gcz.L.gcz_zstd_match_find(ctx.handle, h_in.data_ptr(), n, DEPTH, h_seqs.data_ptr(), nseq + 1024,
+                                       h_off.data_ptr())
+        if rc != 0:
+            raise RuntimeError(gcz.L.gcz_last_error(ctx.handle).decode())
+
+    e2e_step()
+    barrier(dist, torch, local)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    barrier(dist, torch, local)
+    e2e_max = max_over_ranks(dist, torch, e2e_s)
+    e2e_value = world * n * args.e2e_steps / e2e_max / 1e9
+    assert int(h_off[-1].item()) == nseq
+
+    # ---- roofline of the match-find step (match kernel + offset scan + compaction)
+    peak, peak_kind = peaks()
+    step_ms = kern_ms / max(kern_launches, 1)
+    alg_bytes = n + 16 * nseq + 8 * B  # input once + ZSTD_Sequence out + counts/offsets
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get(WORKLOAD)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = data[:256 << 20]
+        dt, _ = cpu_oracle_time(sample, DEPTH, threads)
+        cpu = {"value": round(sample.size / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"first 256 MiB of the same 1 GiB input (4096 windows), oracle/oracle.c on {threads} threads"}
+
+    total_launches = sum_over_ranks(dist, torch, all_launches)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "windows_per_gpu": B, "window": 65536,
+                       "search_depth": DEPTH, "sequences_per_gpu": nseq, "parallelism": f"replicas{world}",
+                       "l2": "input 1 GiB > 126 MB L2, no flush needed"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": n,
+                    "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms_per_step": round(step_ms, 4),
+                         "algorithmic_bytes_per_step": alg_bytes},
+            "cpu_baseline": cpu,
+            "gpu_launches": int(total_launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """Reference arm: the reference's path on this box.  `value` = its CPU
+    restatement (oracle port) on all host threads over a bounded sample of the
+    workload; `reference_kernels_b200` = the reference's own kernels on the GPU."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import gcz
+
+    n = N_BYTES
+    data = gcz.gen_synthetic(SEED, n, 8 << 20)
+    threads = os.cpu_count() or 1
+    sample = data[:256 << 20]
+    times = []
+    for _ in range(max(args.warmup, 1)):
+        cpu_oracle_time(sample[:16 << 20], DEPTH, threads)
+    steps = max(1, min(args.steps, 5))
+    for _ in range(steps):
+        dt, _ = cpu_oracle_time(sample, DEPTH, threads)
+        times.append(dt)
+    value = sample.size * steps / sum(times) / 1e9
+    refk = reference_kernels(data)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": steps,
+        "warmup": max(args.warmup, 1), "ms_per_step": round(sum(times) / steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "window": 65536, "search_depth": DEPTH},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"first 256 MiB of the 1 GiB input, oracle/oracle.c on {threads} threads "
+                                   "(the reference has no CPU match finder; its kernels are timed below)"},
+        "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_kernels_b200": refk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def reference_kernels(data):
+    """The reference's zstd_match_find PTX (JIT on this GPU) over the same
+    1 GiB in one grid (kernel only), and its adapter pattern per 8 MiB chunk
+    (alloc_zeros + H2D + launch + D2H of the sequence buffer) on a sample."""
+    try:
+        from oracle import ref_kernels
+        import torch
+
+        if not ref_kernels.available() or not torch.cuda.is_available():
+            return {"unavailable": "oracle/_ref not built or no GPU"}
+        rk = ref_kernels.RefKernels(0)
+        n = data.size
+        d_in = rk.to_device(data)
+        bufs = rk.zstd_alloc(n)
+        rk.zstd_launch(d_in, n, bufs, DEPTH)  # JIT + warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        rk.zstd_launch(d_in, n, bufs, DEPTH)
+        e1.record()
+        torch.cuda.synchronize()
+        k_ms = e0.elapsed_time(e1)
+        del bufs, d_in
+        torch.cuda.empty_cache()
+        # adapter pattern, 8 MiB chunks (compress_zstd_custom.rs:79-116), first 128 MiB
+        chunk = 8 << 20
+        sample = data[:128 << 20]
+        t0 = time.perf_counter()
+        for off in range(0, sample.size, chunk):
+            part = sample[off:off + chunk]
+            d = rk.to_device(part)
+            b = rk.zstd_alloc(part.size)
+            rk.zstd_launch(d, part.size, b, DEPTH)
+            b[0].cpu()
+            b[2].cpu()
+        torch.cuda.synchronize()
+        a_s = time.perf_counter() - t0
+        return {"kernel_only_gbs": round(n / (k_ms / 1e3) / 1e9, 4), "kernel_ms_1gib": round(k_ms, 3),
+                "adapter_pattern_gbs": round(sample.size / a_s / 1e9, 4),
+                "note": "PTX from the reference's own sources and flags, driver JIT; grid=windows, block=256"}
+    except Exception as e:  # report, never fail the arm
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gcz(args)
+
+
+if __name__ == "__main__":
+    main()

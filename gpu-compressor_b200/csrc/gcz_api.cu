@@ -1,0 +1,555 @@
+// libgcz C ABI (include/gcz.h): context, buffers, host and device entry points.
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "gcz.h"
+#include "gcz_kernels.h"
+
+namespace {
+
+constexpr uint32_t kW = GCZ_WINDOW;
+constexpr uint32_t kMaxSeqs = GCZ_ZSTD_MAX_SEQ_PER_WINDOW;  // chunk_size / 3
+// Host-buffer calls process the input in slices of this many windows so that
+// device memory stays bounded (and copies of one slice overlap another).
+constexpr uint32_t kSliceWindows = 2048;  // 128 MiB of input
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+struct HostBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+};
+
+}  // namespace
+
+struct gcz_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string err;
+    uint32_t *d_status = nullptr;
+    DevBuf in, packed, counts, offsets, seqs, lz_packed, lz_has;
+    HostBuf h_offsets, h_packed;
+    int staged = 1;
+    // profiling
+    bool prof = false;
+    std::vector<EventPair> events;
+    size_t ev_used = 0;
+    uint64_t match_launches = 0, all_launches = 0;
+};
+
+namespace {
+
+int fail(gcz_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define GCZ_CUDA(c, call)                                                                          \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail((c), GCZ_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                 \
+    } while (0)
+
+int ensure_dev(gcz_ctx *c, DevBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return GCZ_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GCZ_ENOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    b.cap = bytes;
+    return GCZ_OK;
+}
+
+int ensure_host(gcz_ctx *c, HostBuf &b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.cap >= bytes) return GCZ_OK;
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMallocHost(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, GCZ_ENOMEM, "cudaMallocHost(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    b.cap = bytes;
+    return GCZ_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+cudaStream_t pick_stream(gcz_ctx *c, void *s) { return s ? static_cast<cudaStream_t>(s) : c->stream; }
+
+// Bracket one match-find launch with events when profiling.
+struct ProfScope {
+    gcz_ctx *c;
+    cudaStream_t st;
+    EventPair *ev = nullptr;
+    ProfScope(gcz_ctx *c_, cudaStream_t s) : c(c_), st(s) {
+        c->match_launches++;
+        if (!c->prof) return;
+        if (c->ev_used == c->events.size()) {
+            if (c->events.size() >= 65536) return;
+            EventPair p;
+            if (cudaEventCreate(&p.a) != cudaSuccess || cudaEventCreate(&p.b) != cudaSuccess) return;
+            c->events.push_back(p);
+        }
+        ev = &c->events[c->ev_used++];
+        cudaEventRecord(ev->a, st);
+    }
+    ~ProfScope() {
+        if (ev) cudaEventRecord(ev->b, st);
+    }
+};
+
+int read_status(gcz_ctx *c, cudaStream_t st) {
+    uint32_t h = 0;
+    GCZ_CUDA(c, cudaMemcpyAsync(&h, c->d_status, 4, cudaMemcpyDeviceToHost, st));
+    GCZ_CUDA(c, cudaStreamSynchronize(st));
+    if (h) {
+        GCZ_CUDA(c, cudaMemsetAsync(c->d_status, 0, 4, st));
+        GCZ_CUDA(c, cudaStreamSynchronize(st));
+        if (h & 2u) return fail(c, GCZ_ECAPACITY, "sequence output capacity exceeded (device status %u)", h);
+        return fail(c, GCZ_EDEVICE, "kernel reported status %u (bounded wait expired)", h);
+    }
+    return GCZ_OK;
+}
+
+size_t nwin(size_t n) { return (n + kW - 1) / kW; }
+
+// Zstd on device memory for one contiguous range of windows: packed sequences
+// into ctx scratch, counts, offsets (num+1, relative), compact expansion.
+int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth, void *d_seqs, uint64_t capacity,
+                     uint64_t *d_offsets, cudaStream_t st) {
+    const size_t nb = nwin(n);
+    int r;
+    if ((r = ensure_dev(c, c->packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, c->counts, nb * 4)) != GCZ_OK) return r;
+    gcz::ZstdLaunch l{};
+    l.src = d_src;
+    l.n = n;
+    l.window = kW;
+    l.num_windows = (uint32_t)nb;
+    l.search_depth = depth;
+    l.max_seqs = kMaxSeqs;
+    l.packed = c->packed.p;
+    l.seq_counts = static_cast<uint32_t *>(c->counts.p);
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    l.staged = c->staged;
+    // The profiled interval covers the whole match-find step: match kernel,
+    // offset scan and compaction into ZSTD_Sequence records.
+    ProfScope ps(c, st);
+    GCZ_CUDA(c, gcz::launch_zstd_match(l, st));
+    GCZ_CUDA(c, gcz::launch_scan_counts(l.seq_counts, (uint32_t)nb, d_offsets, st));
+    GCZ_CUDA(c, gcz::launch_expand_seqs(c->packed.p, l.seq_counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
+                                        c->d_status, c->num_sms, st));
+    c->all_launches += 3;
+    return GCZ_OK;
+}
+
+int lzma_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth, uint32_t *d_packed, uint8_t *d_has,
+                     cudaStream_t st) {
+    const size_t nb = nwin(n);
+    gcz::LzmaLaunch l{};
+    l.src = d_src;
+    l.n = n;
+    l.window = kW;
+    l.num_windows = (uint32_t)nb;
+    l.search_depth = depth;
+    l.max_matches = GCZ_LZMA2_MAX_MATCHES;
+    l.packed = d_packed;
+    l.has_matches = d_has;
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    l.staged = c->staged;
+    {
+        ProfScope ps(c, st);
+        GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
+    }
+    c->all_launches += 1;
+    return GCZ_OK;
+}
+
+bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+}  // namespace
+
+// =========================================================================== context
+
+extern "C" int gcz_create(int device_id, gcz_ctx **out) {
+    if (!out) return GCZ_EINVAL;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device_id < 0 || device_id >= count) {
+        cudaGetLastError();
+        return GCZ_EINVAL;
+    }
+    gcz_ctx *c = new gcz_ctx();
+    c->device = device_id;
+    DeviceGuard g(device_id);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device_id) != cudaSuccess) {
+        delete c;
+        return GCZ_ECUDA;
+    }
+    c->num_sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_status, 16) != cudaSuccess || cudaMemset(c->d_status, 0, 16) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->stream) cudaStreamDestroy(c->stream);
+        delete c;
+        return GCZ_ECUDA;
+    }
+    *out = c;
+    return GCZ_OK;
+}
+
+extern "C" void gcz_destroy(gcz_ctx *c) {
+    if (!c) return;
+    {
+        DeviceGuard g(c->device);
+        cudaStreamSynchronize(c->stream);
+        for (DevBuf *b : {&c->in, &c->packed, &c->counts, &c->offsets, &c->seqs, &c->lz_packed, &c->lz_has})
+            if (b->p) cudaFree(b->p);
+        for (HostBuf *b : {&c->h_offsets, &c->h_packed})
+            if (b->p) cudaFreeHost(b->p);
+        for (auto &e : c->events) {
+            cudaEventDestroy(e.a);
+            cudaEventDestroy(e.b);
+        }
+        if (c->d_status) cudaFree(c->d_status);
+        cudaStreamDestroy(c->stream);
+    }
+    delete c;
+}
+
+extern "C" const char *gcz_last_error(const gcz_ctx *c) { return c ? c->err.c_str() : "null context"; }
+extern "C" int gcz_device(const gcz_ctx *c) { return c ? c->device : -1; }
+extern "C" const char *gcz_version(void) { return "gcz 0.1 (sm_100a)"; }
+
+extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
+    if (!c || !key) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!strcmp(key, "staged")) {
+        c->staged = value ? 1 : 0;
+        return GCZ_OK;
+    }
+    return fail(c, GCZ_EINVAL, "unknown option '%s'", key);
+}
+
+extern "C" int gcz_sync(gcz_ctx *c, void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    return read_status(c, pick_stream(c, stream));
+}
+
+// =========================================================================== Zstd
+
+extern "C" uint32_t gcz_zstd_search_depth_for_level(uint32_t level) {
+    return level == 1 ? 16u : (level == 2 ? 64u : 1u);  // compress_zstd_custom.rs:57-61
+}
+extern "C" size_t gcz_num_windows(size_t n) { return nwin(n); }
+extern "C" size_t gcz_zstd_max_sequences(size_t n) {
+    // A window of s bytes holds at most floor((s-1)/3) sequences (position 0 is
+    // always a literal and every match is >= 3 bytes); never more than the
+    // kernel's per-window stride.
+    size_t total = 0, full = n / kW, rem = n % kW;
+    total = full * std::min<size_t>((kW - 1) / 3, kMaxSeqs);
+    if (rem) total += rem > 1 ? (rem - 1) / 3 : 0;
+    return total;
+}
+
+extern "C" int gcz_zstd_match_find_device(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t search_depth,
+                                          gcz_zstd_sequence *d_seqs, size_t seq_capacity, uint64_t *d_offsets,
+                                          void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!d_src || !d_seqs)) || !d_offsets) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_src)) return fail(c, GCZ_EINVAL, "d_src must be 16-byte aligned");
+    if (nwin(n) > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "input too large");
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    if (n == 0) {
+        GCZ_CUDA(c, cudaMemsetAsync(d_offsets, 0, 8, st));
+        return GCZ_OK;
+    }
+    return zstd_device_core(c, d_src, n, search_depth, d_seqs, seq_capacity, d_offsets, st);
+}
+
+extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
+                                   gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!src || !seqs)) || !offsets) return fail(c, GCZ_EINVAL, "null pointer");
+    DeviceGuard g(c->device);
+    cudaStream_t st = c->stream;
+    const size_t nb = nwin(n);
+    offsets[0] = 0;
+    int r;
+    uint64_t done = 0;  // sequences written so far
+    for (size_t b0 = 0; b0 < nb; b0 += kSliceWindows) {
+        const size_t b1 = std::min(nb, b0 + (size_t)kSliceWindows), sb = b1 - b0;
+        const size_t off = b0 * (size_t)kW, len = std::min(n - off, sb * (size_t)kW);
+        if ((r = ensure_dev(c, c->in, sb * (size_t)kW + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->offsets, (sb + 1) * 8)) != GCZ_OK) return r;
+        const size_t slice_cap = gcz_zstd_max_sequences(len);
+        if ((r = ensure_dev(c, c->seqs, std::max<size_t>(slice_cap, 1) * 16)) != GCZ_OK) return r;
+        if ((r = ensure_host(c, c->h_offsets, (sb + 1) * 8)) != GCZ_OK) return r;
+        GCZ_CUDA(c, cudaMemcpyAsync(c->in.p, src + off, len, cudaMemcpyHostToDevice, st));
+        if ((r = zstd_device_core(c, static_cast<const uint8_t *>(c->in.p), len, search_depth, c->seqs.p, slice_cap,
+                                  static_cast<uint64_t *>(c->offsets.p), st)) != GCZ_OK)
+            return r;
+        uint64_t *ho = static_cast<uint64_t *>(c->h_offsets.p);
+        GCZ_CUDA(c, cudaMemcpyAsync(ho, c->offsets.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, st));
+        if ((r = read_status(c, st)) != GCZ_OK) return r;
+        const uint64_t total = ho[sb];
+        if (done + total > seq_capacity)
+            return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)(done + total),
+                        seq_capacity);
+        if (total)
+            GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, c->seqs.p, total * 16, cudaMemcpyDeviceToHost, st));
+        for (size_t i = 1; i <= sb; i++) offsets[b0 + i] = done + ho[i];
+        done += total;
+        GCZ_CUDA(c, cudaStreamSynchronize(st));
+    }
+    return GCZ_OK;
+}
+
+extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *d_input, uint32_t *d_sequences,
+                                                     uint8_t *d_literals, uint32_t *d_seq_counts,
+                                                     uint32_t *d_lit_counts, uint32_t chunk_size, uint32_t num_chunks,
+                                                     uint32_t total_input_size, uint32_t search_depth,
+                                                     uint32_t max_sequences_per_chunk, void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (chunk_size == 0 || chunk_size > 65536 || (chunk_size & 15u))
+        return fail(c, GCZ_EINVAL, "chunk_size must be a multiple of 16 in [16, 65536]");
+    if (!d_input || !d_sequences || !d_seq_counts) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_input)) return fail(c, GCZ_EINVAL, "d_input must be 16-byte aligned");
+    // Windows past the input (the reference computes a negative size there) are not processed.
+    uint64_t nb = ((uint64_t)total_input_size + chunk_size - 1) / chunk_size;
+    if (nb > num_chunks) nb = num_chunks;
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    gcz::ZstdLaunch l{};
+    l.src = d_input;
+    l.n = std::min<uint64_t>(total_input_size, nb * chunk_size);
+    l.window = chunk_size;
+    l.num_windows = (uint32_t)nb;
+    l.search_depth = search_depth;
+    l.max_seqs = max_sequences_per_chunk;
+    l.ref_seqs = d_sequences;
+    l.seq_counts = d_seq_counts;
+    l.lit_counts = d_lit_counts;
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    l.staged = c->staged;
+    {
+        ProfScope ps(c, st);
+        GCZ_CUDA(c, gcz::launch_zstd_match(l, st));
+    }
+    c->all_launches++;
+    if (d_literals) {
+        GCZ_CUDA(c, gcz::launch_zstd_literals(d_input, l.n, chunk_size, l.num_windows, d_sequences, d_seq_counts,
+                                              max_sequences_per_chunk, d_literals, c->num_sms, st));
+        c->all_launches++;
+    }
+    return GCZ_OK;
+}
+
+// =========================================================================== LZMA2
+
+extern "C" int gcz_lzma2_match_find_device(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t search_depth,
+                                           uint32_t *d_packed, uint8_t *d_has_matches, void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (n && !d_src) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_src)) return fail(c, GCZ_EINVAL, "d_src must be 16-byte aligned");
+    if (nwin(n) > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "input too large");
+    DeviceGuard g(c->device);
+    if (n == 0) return GCZ_OK;
+    return lzma_device_core(c, d_src, n, search_depth, d_packed, d_has_matches, pick_stream(c, stream));
+}
+
+namespace {
+// Host-side slices for the two LZMA2 host entry points.
+template <class Consume>
+int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, uint32_t *packed_out,
+                     uint8_t *has_out, Consume consume) {
+    cudaStream_t st = c->stream;
+    const size_t nb = nwin(n);
+    int r;
+    for (size_t b0 = 0; b0 < nb; b0 += kSliceWindows) {
+        const size_t b1 = std::min(nb, b0 + (size_t)kSliceWindows), sb = b1 - b0;
+        const size_t off = b0 * (size_t)kW, len = std::min(n - off, sb * (size_t)kW);
+        if ((r = ensure_dev(c, c->in, sb * (size_t)kW + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->lz_packed, sb * (size_t)kW * 4)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->lz_has, sb + 16)) != GCZ_OK) return r;
+        GCZ_CUDA(c, cudaMemcpyAsync(c->in.p, src + off, len, cudaMemcpyHostToDevice, st));
+        if ((r = lzma_device_core(c, static_cast<const uint8_t *>(c->in.p), len, depth,
+                                  static_cast<uint32_t *>(c->lz_packed.p), static_cast<uint8_t *>(c->lz_has.p), st)) !=
+            GCZ_OK)
+            return r;
+        uint32_t *dst = packed_out ? packed_out + off : nullptr;
+        if (!dst) {
+            if ((r = ensure_host(c, c->h_packed, sb * (size_t)kW * 4)) != GCZ_OK) return r;
+            dst = static_cast<uint32_t *>(c->h_packed.p);
+        }
+        GCZ_CUDA(c, cudaMemcpyAsync(dst, c->lz_packed.p, len * 4, cudaMemcpyDeviceToHost, st));
+        if (has_out) GCZ_CUDA(c, cudaMemcpyAsync(has_out + b0, c->lz_has.p, sb, cudaMemcpyDeviceToHost, st));
+        if ((r = read_status(c, st)) != GCZ_OK) return r;
+        consume(off, len, dst);
+    }
+    return GCZ_OK;
+}
+}  // namespace
+
+extern "C" int gcz_lzma2_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
+                                    uint32_t *packed, uint8_t *has_matches) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (n && !src) return fail(c, GCZ_EINVAL, "null pointer");
+    DeviceGuard g(c->device);
+    return lzma_host_slices(c, src, n, search_depth, packed, has_matches, [](size_t, size_t, const uint32_t *) {});
+}
+
+extern "C" int gcz_lzma2_find_matches(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t max_matches,
+                                      uint32_t *match_distances, uint32_t *match_lengths, uint32_t *match_counts) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (n && !src) return fail(c, GCZ_EINVAL, "null pointer");
+    if (max_matches == 0) return fail(c, GCZ_EINVAL, "max_matches must be >= 1");
+    DeviceGuard g(c->device);
+    const size_t total_pos = nwin(n) * (size_t)kW;
+    // Zero-fill first (alloc_zeros in the reference), then scatter the found matches.
+    auto zero = [&](uint32_t *p, size_t count) {
+        if (!p) return;
+        const unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; t++)
+            th.emplace_back([=] {
+                const size_t a = count * t / nt, b = count * (t + 1) / nt;
+                memset(p + a, 0, (b - a) * 4);
+            });
+        for (auto &x : th) x.join();
+    };
+    zero(match_counts, total_pos);
+    zero(match_distances, total_pos * max_matches);
+    zero(match_lengths, total_pos * max_matches);
+    return lzma_host_slices(c, src, n, GCZ_LZMA2_SEARCH_DEPTH, nullptr, nullptr,
+                            [&](size_t off, size_t len, const uint32_t *pk) {
+                                for (size_t i = 0; i < len; i++) {
+                                    const uint32_t v = pk[i];
+                                    if (!v) continue;
+                                    const size_t q = off + i;
+                                    if (match_counts) match_counts[q] = 1;
+                                    if (match_distances) match_distances[q * max_matches] = v & 0xFFFFu;
+                                    if (match_lengths) match_lengths[q * max_matches] = v >> 16;
+                                }
+                            });
+}
+
+extern "C" int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *d_input, uint32_t *d_matches,
+                                                      uint32_t *d_match_counts, uint32_t sub_block_size,
+                                                      uint32_t num_sub_blocks, uint32_t total_input_size,
+                                                      uint32_t max_matches_per_pos, uint32_t search_depth,
+                                                      void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (sub_block_size == 0 || sub_block_size > 65536 || (sub_block_size & 15u))
+        return fail(c, GCZ_EINVAL, "sub_block_size must be a multiple of 16 in [16, 65536]");
+    if (max_matches_per_pos == 0) return fail(c, GCZ_EINVAL, "max_matches_per_pos must be >= 1");
+    if (!d_input || !d_matches || !d_match_counts) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_input)) return fail(c, GCZ_EINVAL, "d_input must be 16-byte aligned");
+    uint64_t nb = ((uint64_t)total_input_size + sub_block_size - 1) / sub_block_size;
+    if (nb > num_sub_blocks) nb = num_sub_blocks;
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    gcz::LzmaLaunch l{};
+    l.src = d_input;
+    l.n = std::min<uint64_t>(total_input_size, nb * sub_block_size);
+    l.window = sub_block_size;
+    l.num_windows = (uint32_t)nb;
+    l.search_depth = search_depth;
+    l.max_matches = max_matches_per_pos;
+    l.ref_matches = d_matches;
+    l.ref_counts = d_match_counts;
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    l.staged = c->staged;
+    {
+        ProfScope ps(c, st);
+        GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
+    }
+    c->all_launches++;
+    return GCZ_OK;
+}
+
+// =========================================================================== profiling
+
+extern "C" int gcz_profile_start(gcz_ctx *c) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->prof = true;
+    c->ev_used = 0;
+    c->match_launches = 0;
+    c->all_launches = 0;
+    return GCZ_OK;
+}
+
+extern "C" int gcz_profile_stop(gcz_ctx *c, double *match_kernel_ms, uint64_t *match_kernel_launches,
+                                uint64_t *all_kernel_launches) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    double total = 0.0;
+    for (size_t i = 0; i < c->ev_used; i++) {
+        GCZ_CUDA(c, cudaEventSynchronize(c->events[i].b));
+        float ms = 0.f;
+        GCZ_CUDA(c, cudaEventElapsedTime(&ms, c->events[i].a, c->events[i].b));
+        total += ms;
+    }
+    if (match_kernel_ms) *match_kernel_ms = total;
+    if (match_kernel_launches) *match_kernel_launches = c->match_launches;
+    if (all_kernel_launches) *all_kernel_launches = c->all_launches;
+    c->prof = false;
+    c->ev_used = 0;
+    return GCZ_OK;
+}

@@ -1,0 +1,55 @@
+// Host-side launch interface of the libgcz kernels (internal to the library).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gcz {
+
+struct ZstdLaunch {
+    const uint8_t *src;     // 16-byte aligned
+    uint64_t n;
+    uint32_t window;        // multiple of 16, <= 65536
+    uint32_t num_windows;
+    uint32_t search_depth;
+    uint32_t max_seqs;      // per-window output stride
+    void *packed;           // uint2 per sequence at stride max_seqs (compact path), or null
+    uint32_t *ref_seqs;     // {ll, ml-3, off} triples at stride max_seqs (reference layout), or null
+    uint32_t *seq_counts;
+    uint32_t *lit_counts;   // may be null
+    uint32_t *status;
+    int num_sms;
+    int staged;             // 1: TMA-staged window in shared memory, 0: read through L1
+};
+
+struct LzmaLaunch {
+    const uint8_t *src;
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    uint32_t search_depth;
+    uint32_t max_matches;
+    uint32_t *packed;
+    uint8_t *has_matches;
+    uint32_t *ref_matches;
+    uint32_t *ref_counts;
+    uint32_t *status;
+    int num_sms;
+    int staged;
+};
+
+cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
+cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);
+cudaError_t launch_expand_seqs(const void *packed, const uint32_t *counts, const uint64_t *offsets, uint32_t num,
+                               uint32_t max_seqs, void *out, uint64_t capacity, uint32_t *status, int num_sms,
+                               cudaStream_t st);
+cudaError_t launch_zstd_literals(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows,
+                                 const uint32_t *ref_seqs, const uint32_t *seq_counts, uint32_t max_seqs, uint8_t *lits,
+                                 int num_sms, cudaStream_t st);
+
+cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st);
+cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t window, uint32_t num_windows,
+                               uint32_t max_matches, uint32_t *dists, uint32_t *lens, uint32_t *counts, int num_sms,
+                               cudaStream_t st);
+
+}  // namespace gcz

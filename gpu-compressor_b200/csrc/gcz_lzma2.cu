@@ -1,0 +1,233 @@
+// LZMA2 L1+ match finder for sm_100a.
+//
+// Reproduces lzma2_match_find (lzma2_match_find.cu:54-194) bit for bit.  The
+// reference walks each 64 KiB window with one thread: a one-entry 14-bit table
+// (empty == 0xFFFF), the "chain" loop stops after its first candidate
+// (:157-160), so every position gets at most one match:
+//   - candidate = table entry for hash(q) (q+3 < size), verified on 4 bytes
+//     (len 4, extended to <= min(size-q, 273)) or else on 2 bytes (len 2,
+//     extended the same way, which stops at 3 at most);
+//   - if there is none, a distance-1 run when src[q-1]==src[q]==src[q+1]
+//     (:164-181).
+// Every position with q+3 < size is inserted right after its own lookup, so
+// the candidate at q is cand(q) = max{p < q : hash(p) == hash(q)} (or none):
+// one warp per window computes it 32 positions per step (__match_any_sync for
+// in-step predecessors, shared-memory table for earlier steps) and then every
+// lane verifies and extends its own position independently.
+#include <type_traits>
+
+#include "gcz_common.cuh"
+#include "gcz_kernels.h"
+
+namespace gcz {
+namespace {
+
+constexpr uint32_t kLzmaMaxMatch = 273;  // MAX_MATCH_LEN, lzma2_match_find.cu:21
+constexpr uint32_t kNone = 0xFFFFu;      // empty sentinel, :73
+
+// First index in [len, lim) where the bytes at c+i and q+i differ, else lim.
+template <class Win>
+__device__ __forceinline__ uint32_t extend_lane(const Win &win, uint32_t c, uint32_t q, uint32_t len, uint32_t lim) {
+    while (len < lim) {
+        const uint32_t d = win.u32(q + len) ^ win.u32(c + len);
+        if (d) {
+            len += (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3;
+            return len < lim ? len : lim;
+        }
+        len += 4u;
+    }
+    return lim;
+}
+
+// First index in [len, lim) where byte q+i differs from `b`, else lim.
+template <class Win>
+__device__ __forceinline__ uint32_t run_lane(const Win &win, uint32_t q, uint32_t b, uint32_t len, uint32_t lim) {
+    const uint32_t pat = b * 0x01010101u;
+    while (len < lim) {
+        const uint32_t d = win.u32(q + len) ^ pat;
+        if (d) {
+            len += (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3;
+            return len < lim ? len : lim;
+        }
+        len += 4u;
+    }
+    return lim;
+}
+
+struct LzmaArgs {
+    const uint8_t *src;
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    uint32_t search_depth;   // 0 disables the hash candidate (chain loop never runs)
+    uint32_t max_matches;    // slot stride of the reference layout
+    uint32_t *packed;        // compact: len<<16 | dist per position (or null)
+    uint8_t *has_matches;    // per window (or null)
+    uint32_t *ref_matches;   // reference layout LzmaMatch pairs (or null)
+    uint32_t *ref_counts;    // reference layout counts (or null)
+    uint32_t *status;
+};
+
+template <class Win>
+__device__ void lzma_window(const Win &win, uint16_t *T, uint32_t size, const LzmaArgs &a, uint32_t w) {
+    const uint32_t lane = lane_id();
+    const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
+    {
+        uint32_t *t32 = reinterpret_cast<uint32_t *>(T);
+        for (uint32_t i = lane; i < kHashSize / 2; i += 32) t32[i] = 0xFFFFFFFFu;  // :72-74
+    }
+    __syncwarp();
+    const uint64_t wbase = static_cast<uint64_t>(w) * a.window;
+    uint32_t *packed = a.packed ? a.packed + wbase : nullptr;
+    uint32_t *rc = a.ref_counts ? a.ref_counts + wbase : nullptr;
+    uint32_t *rm = a.ref_matches ? a.ref_matches + wbase * a.max_matches * 2u : nullptr;
+    uint32_t any = 0;
+    const uint32_t nsteps = (size + 31u) >> 5;
+    for (uint32_t s = 0; s < nsteps; ++s) {
+        const uint32_t q = (s << 5) + lane;
+        const bool valid4 = q + 3u < size;
+        const uint32_t x = win.u32(q);
+        const uint32_t h = hash4(x);
+        const uint32_t g = __match_any_sync(kFull, valid4 ? h : (0x80000000u | lane));
+        const uint32_t lower = g & lt;
+        const uint32_t tv = valid4 ? static_cast<uint32_t>(T[h]) : kNone;
+        const uint32_t cand = lower ? ((s << 5) + 31u - static_cast<uint32_t>(__clz(lower))) : tv;
+        __syncwarp();
+        if (valid4 && !(g & gt)) T[h] = static_cast<uint16_t>(q);  // :108
+        __syncwarp();
+
+        uint32_t dist = 0, len = 0;
+        if (q + 1u < size) {
+            if (valid4 && a.search_depth > 0 && cand != kNone) {
+                const uint32_t lim = size - q < kLzmaMaxMatch ? size - q : kLzmaMaxMatch;
+                const uint32_t y = win.u32(cand);
+                uint32_t l = 0;
+                if (y == x) {
+                    l = extend_lane(win, cand, q, 4u, lim);             // :127-133
+                } else if (((y ^ x) & 0xFFFFu) == 0u) {
+                    l = ((y ^ x) & 0xFF0000u) == 0u ? 3u : 2u;          // :134-139 (byte 3 differs)
+                }
+                if (l >= 2u) {
+                    dist = q - cand;
+                    len = l;
+                }
+            }
+            if (len == 0 && q > 0) {  // distance-1 run (:164-181)
+                const uint32_t b0 = x & 0xFFu, b1 = (x >> 8) & 0xFFu;
+                if (b1 == b0 && win.byte(q - 1u) == b0) {
+                    const uint32_t lim = size - q < kLzmaMaxMatch ? size - q : kLzmaMaxMatch;
+                    len = run_lane(win, q, b0, 2u, lim);
+                    dist = 1;
+                }
+            }
+        }
+        if (q < size) {
+            if (packed) packed[q] = len ? ((len << 16) | dist) : 0u;
+            if (rc) rc[q] = len ? 1u : 0u;
+            if (rm && len) {
+                uint32_t *slot = rm + static_cast<uint64_t>(q) * a.max_matches * 2u;
+                slot[0] = dist;
+                slot[1] = len;
+            }
+        }
+        any |= len;
+    }
+    if (rc)
+        for (uint32_t q = size + lane; q < a.window; q += 32) rc[q] = 0u;  // :188-190
+    any = __any_sync(kFull, any != 0);
+    if (a.has_matches && lane == 0) a.has_matches[w] = any ? 1 : 0;
+}
+
+constexpr uint32_t kSmemData = kMaxWindow + 64;
+constexpr uint32_t kSmemTable = kHashSize * sizeof(uint16_t);
+constexpr uint32_t kSmemStaged = kSmemData + kSmemTable + 16;
+
+template <bool kStaged>
+__global__ void __launch_bounds__(32) lzma_match_kernel(LzmaArgs a) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint16_t *T = reinterpret_cast<uint16_t *>(smem + (kStaged ? kSmemData : 0u));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kSmemData + kSmemTable);
+    uint32_t parity = 0;
+    if (kStaged) {
+        if (lane_id() == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+        }
+        __syncwarp();
+    }
+    for (uint32_t w = blockIdx.x; w < a.num_windows; w += gridDim.x) {
+        const uint64_t start = static_cast<uint64_t>(w) * a.window;
+        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        if constexpr (kStaged) {
+            if (!stage_window(smem, a.src + start, size, bar, parity, a.status)) return;
+            SmemWin win{reinterpret_cast<const uint32_t *>(smem)};
+            lzma_window(win, T, size, a, w);
+        } else {
+            GlobalWin win{reinterpret_cast<const uint32_t *>(a.src + start), (size + 3u) >> 2};
+            lzma_window(win, T, size, a, w);
+        }
+    }
+}
+
+// Packed -> GpuMatchData layout (compress_lzma2_custom.rs:539-549): counts,
+// and de-interleaved distance / length arrays with max_matches slots per
+// position, unused slots zero (the reference allocates them with alloc_zeros).
+__global__ void __launch_bounds__(256) lzma_unpack_kernel(const uint32_t *packed, uint64_t n, uint32_t window,
+                                                          uint32_t num_windows, uint32_t max_matches,
+                                                          uint32_t *dists, uint32_t *lens, uint32_t *counts) {
+    const uint64_t total = static_cast<uint64_t>(num_windows) * window;
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        // positions past n inside the last window have count 0
+        const uint32_t v = i < n ? packed[i] : 0u;
+        if (counts) counts[i] = v ? 1u : 0u;
+        const uint64_t base = i * max_matches;
+        for (uint32_t k = 0; k < max_matches; ++k) {
+            if (dists) dists[base + k] = (k == 0) ? (v & 0xFFFFu) : 0u;
+            if (lens) lens[base + k] = (k == 0) ? (v >> 16) : 0u;
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st) {
+    LzmaArgs a{};
+    a.src = l.src;
+    a.n = l.n;
+    a.window = l.window;
+    a.num_windows = l.num_windows;
+    a.search_depth = l.search_depth;
+    a.max_matches = l.max_matches;
+    a.packed = l.packed;
+    a.has_matches = l.has_matches;
+    a.ref_matches = l.ref_matches;
+    a.ref_counts = l.ref_counts;
+    a.status = l.status;
+    if (a.num_windows == 0) return cudaSuccess;
+    const bool staged = l.staged != 0;
+    int grid = l.num_sms * (staged ? 2 : 6);
+    if (static_cast<uint32_t>(grid) > a.num_windows) grid = static_cast<int>(a.num_windows);
+    const uint32_t smem = staged ? kSmemStaged : kSmemTable;
+    cudaError_t e;
+    if (staged) {
+        e = cudaFuncSetAttribute(lzma_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        lzma_match_kernel<true><<<grid, 32, smem, st>>>(a);
+    } else {
+        e = cudaFuncSetAttribute(lzma_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        lzma_match_kernel<false><<<grid, 32, smem, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t window, uint32_t num_windows,
+                               uint32_t max_matches, uint32_t *dists, uint32_t *lens, uint32_t *counts, int num_sms,
+                               cudaStream_t st) {
+    if (num_windows == 0) return cudaSuccess;
+    lzma_unpack_kernel<<<num_sms * 8, 256, 0, st>>>(packed, n, window, num_windows, max_matches, dists, lens, counts);
+    return cudaGetLastError();
+}
+
+}  // namespace gcz

@@ -1,0 +1,168 @@
+/*
+ * gcz.h -- C ABI of libgcz, the B200 (sm_100a) match finders behind
+ * gpu-compressor's Zstd L1/L2 and LZMA2 L1+ levels.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (GCZ_OK == 0, negative on error; gcz_last_error() gives the message).  No
+ * call aborts or traps.  Results are bit-identical to the reference kernels:
+ *
+ *   zstd_match_find    zstd_compress.cu:179-355   (Zstd L1 and L2)
+ *   lzma2_match_find   lzma2_match_find.cu:54-194 (LZMA2 L1+)
+ *
+ * Windows: inputs are cut into independent 64 KiB windows
+ * (CUSTOM_ZSTD_CHUNK_SIZE / LZMA2_CUSTOM_CHUNK_SIZE, constants.rs:5,10); no match
+ * crosses a window.  The last window may be short.
+ *
+ * Host-buffer calls (`const uint8_t *src` is host memory) copy in, run and copy
+ * out internally; when the host buffers are pinned the copies overlap the
+ * kernels.  `_device` calls take device pointers and a cudaStream_t (passed as
+ * void*) and only enqueue work.
+ */
+#ifndef GCZ_H
+#define GCZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GCZ_WINDOW 65536u              /* constants.rs:5 (Zstd), constants.rs:10 (LZMA2) */
+#define GCZ_ZSTD_MAX_SEQ_PER_WINDOW 21845u /* chunk_size / 3, compress_zstd_custom.rs:55 */
+#define GCZ_LZMA2_MAX_MATCHES 8u       /* LZMA2_MAX_MATCHES_PER_POS, constants.rs:12 */
+#define GCZ_LZMA2_SEARCH_DEPTH 32u     /* LZMA2_HC4_SEARCH_DEPTH, constants.rs:13 */
+
+enum {
+    GCZ_OK = 0,
+    GCZ_EINVAL = -1,     /* bad argument (null pointer, size, alignment) */
+    GCZ_ECUDA = -2,      /* a CUDA runtime call failed */
+    GCZ_ENOMEM = -3,     /* device or pinned-host allocation failed */
+    GCZ_ECAPACITY = -4,  /* an output buffer is too small */
+    GCZ_EDEVICE = -5,    /* a kernel reported an error status (bounded wait expired) */
+};
+
+typedef struct gcz_ctx gcz_ctx;
+
+/* ZSTD_Sequence (zstd.h), the record ZSTD_compressSequences consumes.  The
+ * reference builds exactly these on the host from the kernel's {ll, ml-3, off}
+ * triples: offset=off, litLength=ll, matchLength=ml+3, rep=0
+ * (compress_zstd_custom.rs:8-14,137-153). */
+typedef struct {
+    uint32_t offset;
+    uint32_t litLength;
+    uint32_t matchLength;
+    uint32_t rep;
+} gcz_zstd_sequence;
+
+/* ---------------------------------------------------------------- context */
+
+/* Replaces the per-call cudaSetDevice + CudaDevice::new + load_ptx of both
+ * adapters (compress_zstd_custom.rs:63-77, compress_lzma2_custom.rs:494-506):
+ * the context is created once per device and reused; it owns the stream and
+ * device/pinned staging buffers (grown on demand, freed by gcz_destroy). */
+int gcz_create(int device_id, gcz_ctx **out);
+void gcz_destroy(gcz_ctx *ctx);
+const char *gcz_last_error(const gcz_ctx *ctx);
+int gcz_device(const gcz_ctx *ctx);
+const char *gcz_version(void);
+
+/* Schedule-only knobs (they never change results): "staged" = 1 stages each
+ * window into shared memory with bulk copies (default), 0 reads it through L1. */
+int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
+
+/* Synchronise `stream` (NULL = the context's stream) and report any error
+ * status a kernel enqueued by a _device call recorded since the last check
+ * (GCZ_ECAPACITY when a compact output overflowed its capacity). */
+int gcz_sync(gcz_ctx *ctx, void *stream);
+
+/* ---------------------------------------------------------------- Zstd L1/L2 */
+
+/* level -> search_depth exactly as compress_zstd_custom.rs:57-61 (1->16, 2->64,
+ * else 1).  Only search_depth > 1 matters to the kernel (lazy step on/off,
+ * zstd_compress.cu:278), so levels 1 and 2 give identical sequences. */
+uint32_t gcz_zstd_search_depth_for_level(uint32_t level);
+
+size_t gcz_num_windows(size_t n);
+/* Upper bound on the total sequence count for n input bytes. */
+size_t gcz_zstd_max_sequences(size_t n);
+
+/* GPU half of compress_chunk_zstd_custom (compress_zstd_custom.rs:47-153):
+ * the sequences of every 64 KiB window of src[0..n), already converted to
+ * ZSTD_Sequence.  Window b's sequences are seqs[offsets[b] .. offsets[b+1]);
+ * offsets has num_windows+1 entries.  Feeding them with the window's bytes to
+ * ZSTD_compressSequences gives the reference's frames byte for byte. */
+int gcz_zstd_match_find(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t search_depth,
+                        gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets);
+
+/* Same on device memory.  d_src must be 16-byte aligned.  d_seqs needs
+ * gcz_zstd_max_sequences(n) entries (or the actual count), d_offsets
+ * num_windows+1 entries.  Enqueued on `stream` (cudaStream_t; NULL = the
+ * context's stream). */
+int gcz_zstd_match_find_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, uint32_t search_depth,
+                               gcz_zstd_sequence *d_seqs, size_t seq_capacity, uint64_t *d_offsets,
+                               void *stream);
+
+/* Kernel-level drop-in for zstd_match_find (zstd_compress.cu:179-190): same
+ * arguments, same output layout -- {literal_length, match_length-3, offset}
+ * u32 triples at stride max_sequences_per_chunk per window, literal bytes at
+ * stride chunk_size (d_literals may be NULL), per-window counts (d_lit_counts
+ * may be NULL).  chunk_size must be a multiple of 16 and <= 65536. */
+int gcz_zstd_match_find_ref_layout_device(gcz_ctx *ctx, const uint8_t *d_input, uint32_t *d_sequences,
+                                          uint8_t *d_literals, uint32_t *d_seq_counts,
+                                          uint32_t *d_lit_counts, uint32_t chunk_size, uint32_t num_chunks,
+                                          uint32_t total_input_size, uint32_t search_depth,
+                                          uint32_t max_sequences_per_chunk, void *stream);
+
+/* ---------------------------------------------------------------- LZMA2 L1+ */
+
+/* Packed per-position result: 0 when the position has no match, else
+ * (length << 16) | distance.  The reference records at most one match per
+ * position (its chain loop stops after the first candidate,
+ * lzma2_match_find.cu:157-160), so this holds everything it finds. */
+#define GCZ_LZMA2_DIST(p) ((p) & 0xFFFFu)
+#define GCZ_LZMA2_LEN(p) ((p) >> 16)
+
+/* Compact form: packed[q] for every q < n (n entries), and has_matches[b]
+ * (num_windows bytes, 0/1) = any(match_counts > 0) over window b -- the one bit
+ * encode_single_sub_block consumes (compress_lzma2_custom.rs:577).  Either
+ * output may be NULL. */
+int gcz_lzma2_match_find(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t search_depth,
+                         uint32_t *packed, uint8_t *has_matches);
+int gcz_lzma2_match_find_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, uint32_t search_depth,
+                                uint32_t *d_packed, uint8_t *d_has_matches, void *stream);
+
+/* gpu_find_matches (compress_lzma2_custom.rs:483-560): the GpuMatchData arrays,
+ * de-interleaved and zero-filled exactly like the reference's alloc_zeros +
+ * split loop: match_counts[b*W + q], match_distances / match_lengths at
+ * [(b*W + q)*max_matches + k].  W = 65536.  Any output may be NULL. */
+int gcz_lzma2_find_matches(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t max_matches,
+                           uint32_t *match_distances, uint32_t *match_lengths, uint32_t *match_counts);
+
+/* Kernel-level drop-in for lzma2_match_find (lzma2_match_find.cu:54-63): same
+ * arguments and layout -- LzmaMatch{distance,length} u32 pairs at
+ * [(b*sub_block_size + q)*max_matches_per_pos + k] and match_counts[b*sub_block_size + q].
+ * Slots past a position's count are not written (the reference host zero-fills
+ * them).  sub_block_size must be a multiple of 16 and <= 65536. */
+int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *ctx, const uint8_t *d_input, uint32_t *d_matches,
+                                           uint32_t *d_match_counts, uint32_t sub_block_size,
+                                           uint32_t num_sub_blocks, uint32_t total_input_size,
+                                           uint32_t max_matches_per_pos, uint32_t search_depth,
+                                           void *stream);
+
+/* ---------------------------------------------------------------- timing */
+
+/* Between gcz_profile_start and gcz_profile_stop every match-find step this
+ * context launches is bracketed by CUDA events on its own launch stream.
+ * gcz_profile_stop synchronises those events and returns the summed device
+ * time of the match-find kernels, their launch count, and the count of all
+ * kernels the library launched in that interval (match-find + compaction). */
+int gcz_profile_start(gcz_ctx *ctx);
+int gcz_profile_stop(gcz_ctx *ctx, double *match_kernel_ms, uint64_t *match_kernel_launches,
+                     uint64_t *all_kernel_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GCZ_H */
