@@ -15,6 +15,8 @@ GCZ_ECUDA = -2
 GCZ_ENOMEM = -3
 GCZ_ECAPACITY = -4
 GCZ_EDEVICE = -5
+GCZ_ETOOLARGE = -6
+NOALLOC_MAX_INPUT = 8 << 20
 
 WINDOW = 65536
 ZSTD_MAX_SEQ_PER_WINDOW = 21845
@@ -37,6 +39,7 @@ SIGNATURES = {
     "gcz_zstd_max_sequences": (_sz, [_sz]),
     "gcz_zstd_match_find": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp]),
     "gcz_zstd_match_find_device": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp, _vp]),
+    "gcz_zstd_match_find_device_noalloc": (_i, [_i, _vp, _sz, _u32, _vp, _sz, _vp, _vp]),
     "gcz_zstd_match_find_ref_layout_device": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp]),
     "gcz_lzma2_match_find": (_i, [_vp, _vp, _sz, _u32, _vp, _vp]),
     "gcz_lzma2_match_find_device": (_i, [_vp, _vp, _sz, _u32, _vp, _vp, _vp]),

@@ -40,6 +40,7 @@ enum {
     GCZ_ENOMEM = -3,     /* device or pinned-host allocation failed */
     GCZ_ECAPACITY = -4,  /* an output buffer is too small */
     GCZ_EDEVICE = -5,    /* a kernel reported an error status (bounded wait expired) */
+    GCZ_ETOOLARGE = -6,  /* input larger than gcz_zstd_match_find_device_noalloc's static scratch */
 };
 
 typedef struct gcz_ctx gcz_ctx;
@@ -102,6 +103,28 @@ int gcz_zstd_match_find(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t sea
 int gcz_zstd_match_find_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, uint32_t search_depth,
                                gcz_zstd_sequence *d_seqs, size_t seq_capacity, uint64_t *d_offsets,
                                void *stream);
+
+/* No counterpart in the reference.  The Zstd step of
+ * gcz_zstd_match_find_device without any device allocation, for callers that
+ * cannot allocate device memory when they call in: a process whose device
+ * memory is already carved up by another allocator (a serving engine's or a
+ * framework's reserved pool, where one more cudaMalloc can fail or fragment
+ * it), a latency-bound loop that cudaMalloc / cudaFree would stall (cudaFree
+ * synchronises the whole device), or code that cannot hold a gcz_ctx, since
+ * gcz_create itself allocates.  Its scratch is a file-scope device array of
+ * about 21.3 MiB that every GPU loading this library keeps until exit; inputs
+ * above GCZ_NOALLOC_MAX_INPUT (8 MiB, one ZSTD_CHUNK_SIZE pipeline chunk) are
+ * rejected with GCZ_ETOOLARGE.  The caller passes device memory for input and
+ * outputs, as for gcz_zstd_match_find_device; `stream` is a cudaStream_t (NULL
+ * = the legacy default stream) and the call returns once the work on it is
+ * done, with GCZ_ECAPACITY when d_seqs was too small.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) for that
+ * device, so make that first call before any stream capture.  All calls on a
+ * device share the one array: calls that overlap on the GPU race. */
+#define GCZ_NOALLOC_MAX_INPUT (8u << 20)
+int gcz_zstd_match_find_device_noalloc(int device, const uint8_t *d_src, size_t n, uint32_t search_depth,
+                                       gcz_zstd_sequence *d_seqs, size_t seq_capacity, uint64_t *d_offsets,
+                                       void *stream);
 
 /* Kernel-level drop-in for zstd_match_find (zstd_compress.cu:179-190): same
  * arguments, same output layout -- {literal_length, match_length-3, offset}
