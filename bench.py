@@ -47,8 +47,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gcz", choices=["gcz", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
+    ap.add_argument("--bytes", type=int, default=N_BYTES, help="input bytes per GPU (profiling runs use less)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--algo", type=int, default=2, help="1: fused single-warp kernels, 2: sweep + second stage")
     return ap.parse_args()
 
 
@@ -167,11 +169,14 @@ def run_gcz(args):
     world, rank, local, dist = dist_setup(args)
     dev = torch.device("cuda", local)
     ctx = gcz.Context(local)
-    n = N_BYTES
+    ctx.set_option("algo", args.algo)
+    n = args.bytes
     data = gcz.gen_synthetic(SEED + 1000 * rank, n, 8 << 20)
     B = gcz.num_windows(n)
     d_in = torch.from_numpy(data).to(dev)
-    cap = int(gcz.L.gcz_zstd_max_sequences(n))
+    # Output capacity: 4 bytes of records per input byte is ample for this input
+    # (about one sequence per 50 bytes); an overflow would raise in ctx.sync.
+    cap = min(int(gcz.L.gcz_zstd_max_sequences(n)), max(n // 4, 1024))
     d_seqs = torch.empty((cap, 4), dtype=torch.int32, device=dev)
     d_off = torch.empty(B + 1, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -203,26 +208,28 @@ def run_gcz(args):
     value = world * n * args.steps / (ms_max / 1e3) / 1e9
 
     # ---- end-to-end through the host-buffer C-ABI call (pinned buffers)
-    h_in = torch.from_numpy(data).pin_memory()
-    h_seqs = torch.empty((nseq + 1024, 4), dtype=torch.int32).pin_memory()
-    h_off = torch.empty(B + 1, dtype=torch.int64).pin_memory()
+    e2e_value = None
+    if args.e2e_steps > 0:
+        h_in = torch.from_numpy(data).pin_memory()
+        h_seqs = torch.empty((nseq + 1024, 4), dtype=torch.int32).pin_memory()
+        h_off = torch.empty(B + 1, dtype=torch.int64).pin_memory()
 
-    def e2e_step():
-        rc = gcz.L.gcz_zstd_match_find(ctx.handle, h_in.data_ptr(), n, DEPTH, h_seqs.data_ptr(), nseq + 1024,
-                                       h_off.data_ptr())
-        if rc != 0:
-            raise RuntimeError(gcz.L.gcz_last_error(ctx.handle).decode())
+        def e2e_step():
+            rc = gcz.L.gcz_zstd_match_find(ctx.handle, h_in.data_ptr(), n, DEPTH, h_seqs.data_ptr(), nseq + 1024,
+                                           h_off.data_ptr())
+            if rc != 0:
+                raise RuntimeError(gcz.L.gcz_last_error(ctx.handle).decode())
 
-    e2e_step()
-    barrier(dist, torch, local)
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
         e2e_step()
-    e2e_s = time.perf_counter() - t0
-    barrier(dist, torch, local)
-    e2e_max = max_over_ranks(dist, torch, e2e_s)
-    e2e_value = world * n * args.e2e_steps / e2e_max / 1e9
-    assert int(h_off[-1].item()) == nseq
+        barrier(dist, torch, local)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e2e_s = time.perf_counter() - t0
+        barrier(dist, torch, local)
+        e2e_max = max_over_ranks(dist, torch, e2e_s)
+        e2e_value = round(world * n * args.e2e_steps / e2e_max / 1e9, 3)
+        assert int(h_off[-1].item()) == nseq
 
     # ---- roofline of the match-find step (match kernel + offset scan + compaction)
     peak, peak_kind = peaks()
@@ -251,8 +258,9 @@ def run_gcz(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
             "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "windows_per_gpu": B, "window": 65536,
                        "search_depth": DEPTH, "sequences_per_gpu": nseq, "parallelism": f"replicas{world}",
+                       "algo": args.algo, "fallback_windows": ctx.query("fallback_windows"),
                        "l2": "input 1 GiB > 126 MB L2, no flush needed"},
-            "e2e": {"value": round(e2e_value, 3), "unit": "GB/s", "h2d_bytes_per_step": n,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n,
                     "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,

@@ -41,9 +41,11 @@ struct gcz_ctx {
     std::mutex mu;
     std::string err;
     uint32_t *d_status = nullptr;
-    DevBuf in, packed, counts, offsets, seqs, lz_packed, lz_has;
+    DevBuf in, packed, counts, offsets, seqs, lz_packed, lz_has, cand, seg;
     HostBuf h_offsets, h_packed;
     int staged = 1;
+    int algo = 2;          // 1: fused single-warp kernels, 2: candidate sweep + second stage
+    int parse_ctas = 3;    // second-stage CTAs per SM
     // profiling
     bool prof = false;
     std::vector<EventPair> events;
@@ -160,26 +162,68 @@ int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
     int r;
     if ((r = ensure_dev(c, c->packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
     if ((r = ensure_dev(c, c->counts, nb * 4)) != GCZ_OK) return r;
-    gcz::ZstdLaunch l{};
-    l.src = d_src;
-    l.n = n;
-    l.window = kW;
-    l.num_windows = (uint32_t)nb;
-    l.search_depth = depth;
-    l.max_seqs = kMaxSeqs;
-    l.packed = c->packed.p;
-    l.seq_counts = static_cast<uint32_t *>(c->counts.p);
-    l.status = c->d_status;
-    l.num_sms = c->num_sms;
-    l.staged = c->staged;
-    // The profiled interval covers the whole match-find step: match kernel,
-    // offset scan and compaction into ZSTD_Sequence records.
+    uint32_t *counts = static_cast<uint32_t *>(c->counts.p);
+    if (c->algo == 2) {
+        if ((r = ensure_dev(c, c->cand, n * 2 + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
+    }
+    // The profiled interval covers the whole match-find step (all its kernels).
     ProfScope ps(c, st);
-    GCZ_CUDA(c, gcz::launch_zstd_match(l, st));
-    GCZ_CUDA(c, gcz::launch_scan_counts(l.seq_counts, (uint32_t)nb, d_offsets, st));
-    GCZ_CUDA(c, gcz::launch_expand_seqs(c->packed.p, l.seq_counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
+    if (c->algo == 2) {
+        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st));
+        gcz::Zstd2Launch l{};
+        l.src = d_src;
+        l.cand = cand;
+        l.n = n;
+        l.window = kW;
+        l.num_windows = (uint32_t)nb;
+        l.search_depth = depth;
+        l.max_seqs = kMaxSeqs;
+        l.seg = c->seg.p;
+        l.packed = c->packed.p;
+        l.seq_counts = counts;
+        l.status = c->d_status;
+        l.num_sms = c->num_sms;
+        l.ctas_per_sm = c->parse_ctas;
+        GCZ_CUDA(c, gcz::launch_zstd_parse(l, st));
+        c->all_launches += 2;
+    } else {
+        gcz::ZstdLaunch l{};
+        l.src = d_src;
+        l.n = n;
+        l.window = kW;
+        l.num_windows = (uint32_t)nb;
+        l.search_depth = depth;
+        l.max_seqs = kMaxSeqs;
+        l.packed = c->packed.p;
+        l.seq_counts = counts;
+        l.status = c->d_status;
+        l.num_sms = c->num_sms;
+        l.staged = c->staged;
+        GCZ_CUDA(c, gcz::launch_zstd_match(l, st));
+        c->all_launches += 1;
+    }
+    GCZ_CUDA(c, gcz::launch_scan_counts(counts, (uint32_t)nb, d_offsets, st));
+    GCZ_CUDA(c, gcz::launch_expand_seqs(c->packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
                                         c->d_status, c->num_sms, st));
-    c->all_launches += 3;
+    c->all_launches += 2;
+    return GCZ_OK;
+}
+
+int lzma_run(gcz_ctx *c, const gcz::LzmaLaunch &l, cudaStream_t st) {
+    int r;
+    ProfScope ps(c, st);
+    if (c->algo == 2) {
+        if ((r = ensure_dev(c, c->cand, l.n * 2 + 64)) != GCZ_OK) return r;
+        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st));
+        GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, st));
+        c->all_launches += 2;
+    } else {
+        GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
+        c->all_launches += 1;
+    }
     return GCZ_OK;
 }
 
@@ -198,12 +242,7 @@ int lzma_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
     l.status = c->d_status;
     l.num_sms = c->num_sms;
     l.staged = c->staged;
-    {
-        ProfScope ps(c, st);
-        GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
-    }
-    c->all_launches += 1;
-    return GCZ_OK;
+    return lzma_run(c, l, st);
 }
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -245,7 +284,8 @@ extern "C" void gcz_destroy(gcz_ctx *c) {
     {
         DeviceGuard g(c->device);
         cudaStreamSynchronize(c->stream);
-        for (DevBuf *b : {&c->in, &c->packed, &c->counts, &c->offsets, &c->seqs, &c->lz_packed, &c->lz_has})
+        for (DevBuf *b : {&c->in, &c->packed, &c->counts, &c->offsets, &c->seqs, &c->lz_packed, &c->lz_has, &c->cand,
+                          &c->seg})
             if (b->p) cudaFree(b->p);
         for (HostBuf *b : {&c->h_offsets, &c->h_packed})
             if (b->p) cudaFreeHost(b->p);
@@ -270,7 +310,32 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->staged = value ? 1 : 0;
         return GCZ_OK;
     }
+    if (!strcmp(key, "algo") && (value == 1 || value == 2)) {
+        c->algo = (int)value;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "parse_ctas") && value >= 1 && value <= 8) {
+        c->parse_ctas = (int)value;
+        return GCZ_OK;
+    }
     return fail(c, GCZ_EINVAL, "unknown option '%s'", key);
+}
+
+extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
+    if (!c || !key || !value) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!strcmp(key, "algo")) {
+        *value = c->algo;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "fallback_windows")) {  // windows whose speculative parse fell back (since creation)
+        DeviceGuard g(c->device);
+        uint32_t h[2] = {0, 0};
+        GCZ_CUDA(c, cudaMemcpy(h, c->d_status, 8, cudaMemcpyDeviceToHost));
+        *value = (long)h[1];
+        return GCZ_OK;
+    }
+    return fail(c, GCZ_EINVAL, "unknown key '%s'", key);
 }
 
 extern "C" int gcz_sync(gcz_ctx *c, void *stream) {
@@ -368,26 +433,51 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
     if (nb > num_chunks) nb = num_chunks;
     DeviceGuard g(c->device);
     cudaStream_t st = pick_stream(c, stream);
-    gcz::ZstdLaunch l{};
-    l.src = d_input;
-    l.n = std::min<uint64_t>(total_input_size, nb * chunk_size);
-    l.window = chunk_size;
-    l.num_windows = (uint32_t)nb;
-    l.search_depth = search_depth;
-    l.max_seqs = max_sequences_per_chunk;
-    l.ref_seqs = d_sequences;
-    l.seq_counts = d_seq_counts;
-    l.lit_counts = d_lit_counts;
-    l.status = c->d_status;
-    l.num_sms = c->num_sms;
-    l.staged = c->staged;
-    {
+    uint64_t n_eff = std::min<uint64_t>(total_input_size, nb * chunk_size);
+    if (c->algo == 2) {
+        int r;
+        if ((r = ensure_dev(c, c->cand, n_eff * 2 + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
+        ProfScope ps(c, st);
+        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        GCZ_CUDA(c, gcz::launch_cand_sweep(d_input, n_eff, chunk_size, (uint32_t)nb, cand, c->num_sms, st));
+        gcz::Zstd2Launch l{};
+        l.src = d_input;
+        l.cand = cand;
+        l.n = n_eff;
+        l.window = chunk_size;
+        l.num_windows = (uint32_t)nb;
+        l.search_depth = search_depth;
+        l.max_seqs = max_sequences_per_chunk;
+        l.seg = c->seg.p;
+        l.ref_seqs = d_sequences;
+        l.seq_counts = d_seq_counts;
+        l.lit_counts = d_lit_counts;
+        l.status = c->d_status;
+        l.num_sms = c->num_sms;
+        l.ctas_per_sm = c->parse_ctas;
+        GCZ_CUDA(c, gcz::launch_zstd_parse(l, st));
+        c->all_launches += 2;
+    } else {
+        gcz::ZstdLaunch l{};
+        l.src = d_input;
+        l.n = n_eff;
+        l.window = chunk_size;
+        l.num_windows = (uint32_t)nb;
+        l.search_depth = search_depth;
+        l.max_seqs = max_sequences_per_chunk;
+        l.ref_seqs = d_sequences;
+        l.seq_counts = d_seq_counts;
+        l.lit_counts = d_lit_counts;
+        l.status = c->d_status;
+        l.num_sms = c->num_sms;
+        l.staged = c->staged;
         ProfScope ps(c, st);
         GCZ_CUDA(c, gcz::launch_zstd_match(l, st));
+        c->all_launches++;
     }
-    c->all_launches++;
     if (d_literals) {
-        GCZ_CUDA(c, gcz::launch_zstd_literals(d_input, l.n, chunk_size, l.num_windows, d_sequences, d_seq_counts,
+        GCZ_CUDA(c, gcz::launch_zstd_literals(d_input, n_eff, chunk_size, (uint32_t)nb, d_sequences, d_seq_counts,
                                               max_sequences_per_chunk, d_literals, c->num_sms, st));
         c->all_launches++;
     }
@@ -514,12 +604,7 @@ extern "C" int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *c, const uint8_t 
     l.status = c->d_status;
     l.num_sms = c->num_sms;
     l.staged = c->staged;
-    {
-        ProfScope ps(c, st);
-        GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
-    }
-    c->all_launches++;
-    return GCZ_OK;
+    return lzma_run(c, l, st);
 }
 
 // =========================================================================== profiling

@@ -38,7 +38,30 @@ struct LzmaLaunch {
     int staged;
 };
 
+// Second-stage Zstd parse after the candidate sweep.
+struct Zstd2Launch {
+    const uint8_t *src;
+    const uint16_t *cand;   // from launch_cand_sweep
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    uint32_t search_depth;
+    uint32_t max_seqs;
+    void *seg;              // zstd2_seg_scratch_entries(num_windows) uint2 entries
+    void *packed;           // uint2 per sequence at stride max_seqs, or null
+    uint32_t *ref_seqs;     // reference triples at stride max_seqs, or null
+    uint32_t *seq_counts;
+    uint32_t *lit_counts;   // may be null
+    uint32_t *status;       // [0] error bits, [1] windows that took the exact fallback
+    int num_sms;
+    int ctas_per_sm;
+};
+
 cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
+cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
+                              int num_sms, cudaStream_t st);
+size_t zstd2_seg_scratch_entries(uint32_t num_windows);
+cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st);
 cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);
 cudaError_t launch_expand_seqs(const void *packed, const uint32_t *counts, const uint64_t *offsets, uint32_t num,
                                uint32_t max_seqs, void *out, uint64_t capacity, uint32_t *status, int num_sms,
@@ -48,6 +71,7 @@ cudaError_t launch_zstd_literals(const uint8_t *src, uint64_t n, uint32_t window
                                  int num_sms, cudaStream_t st);
 
 cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st);
+cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaStream_t st);
 cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t window, uint32_t num_windows,
                                uint32_t max_matches, uint32_t *dists, uint32_t *lens, uint32_t *counts, int num_sms,
                                cudaStream_t st);

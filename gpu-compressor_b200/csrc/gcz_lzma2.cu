@@ -189,6 +189,134 @@ __global__ void __launch_bounds__(256) lzma_unpack_kernel(const uint32_t *packed
     }
 }
 
+// ---------------------------------------------------------------------------
+// Second stage after the candidate sweep (gcz_sweep.cu): the window is staged
+// into shared memory, cand(q) streams in from global memory, and every lane
+// verifies its own position.  Lengths use the structure of match runs: when
+// cand(q) == cand(q-1)+1 and both positions match on 4 bytes, the common run
+// at q is the one at q-1 shortened by one, so only the first lane of each run
+// (its head) extends, up to min(size-q, 273+31) bytes, and the other lanes of
+// the run derive min(273, E_head - (q - head)) from it -- the same value the
+// reference's per-position loop computes with its 273 cap.
+constexpr uint32_t kL2Threads = 256;
+constexpr uint32_t kL2Pre = 64;
+constexpr uint32_t kL2DataBytes = kL2Pre + kMaxWindow + 64;
+
+struct L2Smem {
+    uint8_t data[kL2DataBytes];
+    uint32_t any;
+    uint32_t flags;
+    alignas(8) uint64_t bar;
+};
+
+struct L2Args {
+    const uint8_t *src;
+    const uint16_t *cand;
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    uint32_t search_depth;
+    uint32_t max_matches;
+    uint32_t *packed;
+    uint8_t *has_matches;
+    uint32_t *ref_matches;
+    uint32_t *ref_counts;
+    uint32_t *status;
+};
+
+__global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    L2Smem &S = *reinterpret_cast<L2Smem *>(smem_raw);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
+    uint32_t parity = 0;
+    if (tid == 0) {
+        mbar_init(&S.bar, 1);
+        fence_mbar_init();
+    }
+    for (uint32_t i = tid; i < kL2Pre / 4; i += kL2Threads) reinterpret_cast<uint32_t *>(S.data)[i] = 0u;
+    __syncthreads();
+    SmemWin win{reinterpret_cast<const uint32_t *>(S.data + kL2Pre)};
+    for (uint32_t wi = blockIdx.x; wi < a.num_windows; wi += gridDim.x) {
+        const uint64_t start = static_cast<uint64_t>(wi) * a.window;
+        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        __syncthreads();
+        if (tid == 0) {
+            S.any = 0;
+            S.flags = 0;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            if (!stage_window(S.data + kL2Pre, a.src + start, size, &S.bar, parity, a.status) && lane == 0)
+                S.flags = 1u;
+        }
+        __syncthreads();
+        if (S.flags) return;
+        const uint16_t *cand = a.cand + start;
+        uint32_t *packed = a.packed ? a.packed + start : nullptr;
+        uint32_t *rc = a.ref_counts ? a.ref_counts + start : nullptr;
+        uint32_t *rm = a.ref_matches ? a.ref_matches + start * a.max_matches * 2u : nullptr;
+        uint32_t any = 0;
+        const uint32_t nsteps = (size + 31u) >> 5;
+        for (uint32_t st = warp; st < nsteps; st += kL2Threads / 32) {
+            const uint32_t q = st * 32u + lane;
+            const bool inwin = q < size;
+            const bool valid4 = q + 3u < size;
+            const uint32_t x = win.u32(q);
+            const uint32_t c = valid4 ? static_cast<uint32_t>(cand[q]) : kNone;
+            const bool has = valid4 && a.search_depth > 0 && c != kNone;
+            const uint32_t y = has ? win.u32(c) : ~x;
+            const bool eq4 = has && y == x;
+            // run structure inside the step
+            const uint32_t c_prev = __shfl_up_sync(kFull, c, 1);
+            const uint32_t eq4_bits = __ballot_sync(kFull, eq4);
+            const bool cont = lane > 0 && eq4 && ((eq4_bits >> (lane - 1)) & 1u) && c == c_prev + 1u;
+            const uint32_t heads = __ballot_sync(kFull, !cont);
+            const uint32_t head = 31u - static_cast<uint32_t>(__clz(heads & (lt | (1u << lane))));
+            uint32_t ext = 0;
+            if (eq4 && !cont) {
+                const uint32_t bound = size - q < kLzmaMaxMatch + 31u ? size - q : kLzmaMaxMatch + 31u;
+                ext = extend_lane(win, c, q, 4u, bound);
+            }
+            const uint32_t ext_head = __shfl_sync(kFull, ext, head);
+            uint32_t dist = 0, len = 0;
+            if (inwin && q + 1u < size) {
+                if (eq4) {
+                    const uint32_t e = ext_head - (lane - head);
+                    len = e < kLzmaMaxMatch ? e : kLzmaMaxMatch;
+                    dist = q - c;
+                } else if (has && ((y ^ x) & 0xFFFFu) == 0u) {
+                    len = ((y ^ x) & 0xFF0000u) == 0u ? 3u : 2u;  // :134-139 (byte 3 differs)
+                    dist = q - c;
+                }
+                if (len == 0 && q > 0) {  // distance-1 run (:164-181)
+                    const uint32_t b0 = x & 0xFFu, b1 = (x >> 8) & 0xFFu;
+                    if (b1 == b0 && win.byte(q - 1u) == b0) {
+                        const uint32_t lim = size - q < kLzmaMaxMatch ? size - q : kLzmaMaxMatch;
+                        len = run_lane(win, q, b0, 2u, lim);
+                        dist = 1;
+                    }
+                }
+            }
+            if (inwin) {
+                if (packed) packed[q] = len ? ((len << 16) | dist) : 0u;
+                if (rc) rc[q] = len ? 1u : 0u;
+                if (rm && len) {
+                    uint32_t *slot = rm + static_cast<uint64_t>(q) * a.max_matches * 2u;
+                    slot[0] = dist;
+                    slot[1] = len;
+                }
+            }
+            any |= len;
+        }
+        if (rc)
+            for (uint32_t q = size + tid; q < a.window; q += kL2Threads) rc[q] = 0u;  // :188-190
+        if (__any_sync(kFull, any != 0) && lane == 0) S.any = 1u;
+        __syncthreads();
+        if (tid == 0 && a.has_matches) a.has_matches[wi] = S.any ? 1 : 0;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st) {
@@ -227,6 +355,30 @@ cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t wind
                                cudaStream_t st) {
     if (num_windows == 0) return cudaSuccess;
     lzma_unpack_kernel<<<num_sms * 8, 256, 0, st>>>(packed, n, window, num_windows, max_matches, dists, lens, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaStream_t st) {
+    if (l.num_windows == 0) return cudaSuccess;
+    L2Args a{};
+    a.src = l.src;
+    a.cand = cand;
+    a.n = l.n;
+    a.window = l.window;
+    a.num_windows = l.num_windows;
+    a.search_depth = l.search_depth;
+    a.max_matches = l.max_matches;
+    a.packed = l.packed;
+    a.has_matches = l.has_matches;
+    a.ref_matches = l.ref_matches;
+    a.ref_counts = l.ref_counts;
+    a.status = l.status;
+    const uint32_t smem = sizeof(L2Smem);
+    cudaError_t e = cudaFuncSetAttribute(lzma_verify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int grid = l.num_sms * 3;
+    if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
+    lzma_verify_kernel<<<grid, kL2Threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 

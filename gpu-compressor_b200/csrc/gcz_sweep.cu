@@ -1,0 +1,96 @@
+// Candidate sweep shared by the Zstd and LZMA2 match finders.
+//
+// Both reference kernels keep a one-entry 14-bit table per 64 KiB window and
+// write every position p with p+3 < size into it exactly once, in increasing
+// order, each lookup at q happening after all p < q were written
+// (zstd_compress.cu:231-235,280,303,328-331; lzma2_match_find.cu:104-108).  The
+// candidate either of them sees at q is therefore
+//     cand(q) = max{ p < q : hash4(p) == hash4(q) }       (0xFFFF if none)
+// which this kernel computes for every position of every window; the match
+// finders then verify, extend and parse from it.
+//
+// One warp sweeps one window 32 positions per step: __match_any_sync groups
+// the lanes with equal hashes (the in-step predecessor is the next lower lane
+// of the group), the window's table in shared memory supplies the last
+// position of earlier steps, and the highest lane of each group writes it
+// back.  Only the table lives in shared memory (32 KiB), so seven windows are
+// swept per SM; the input streams through coalesced 128-byte loads.
+#include "gcz_common.cuh"
+#include "gcz_kernels.h"
+
+namespace gcz {
+namespace {
+
+constexpr int kSweepWarpsPerCta = 7;  // 7 x 32 KiB tables per SM
+
+struct SweepArgs {
+    const uint8_t *src;
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    uint16_t *cand;  // one entry per input byte, same offsets as src
+};
+
+__global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(SweepArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint16_t *T = reinterpret_cast<uint16_t *>(smem) + warp * kHashSize;
+    uint4 *T4 = reinterpret_cast<uint4 *>(T);
+    const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
+    const uint32_t gwarps = gridDim.x * kSweepWarpsPerCta;
+    for (uint32_t w = blockIdx.x * kSweepWarpsPerCta + warp; w < a.num_windows; w += gwarps) {
+        const uint64_t start = static_cast<uint64_t>(w) * a.window;
+        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        for (uint32_t i = lane; i < kHashSize * 2 / 16; i += 32) T4[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        __syncwarp();
+        const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);
+        const uint32_t nwords = (size + 3u) >> 2;
+        uint16_t *out = a.cand + start;
+        // 128-byte blocks: lane l holds word l; the next block is prefetched.
+        uint32_t cur = lane < nwords ? __ldg(src32 + lane) : 0u;
+        for (uint32_t blk = 0; blk * 128u < size; ++blk) {
+            const uint32_t nw = (blk + 1u) * 32u + lane;
+            const uint32_t nxt = nw < nwords ? __ldg(src32 + nw) : 0u;
+            const uint32_t up = __shfl_down_sync(kFull, cur, 1);
+            const uint32_t n0 = __shfl_sync(kFull, nxt, 0);
+            const uint32_t cur1 = lane == 31u ? n0 : up;  // word l+1
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t q = blk * 128u + j * 32u + lane;
+                const uint32_t src_lane = j * 8u + (lane >> 2);
+                const uint32_t lo = __shfl_sync(kFull, cur, src_lane);
+                const uint32_t hi = __shfl_sync(kFull, cur1, src_lane);
+                const uint32_t x = __funnelshift_r(lo, hi, (lane & 3u) * 8u);
+                const bool valid = q + 3u < size;
+                const uint32_t h = hash4(x);
+                const uint32_t g = __match_any_sync(kFull, valid ? h : (0x80000000u | lane));
+                const uint32_t lower = g & lt;
+                const uint32_t tv = valid ? static_cast<uint32_t>(T[h]) : 0xFFFFu;
+                const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv;
+                __syncwarp();
+                if (valid && !(g & gt)) T[h] = static_cast<uint16_t>(q);
+                __syncwarp();
+                if (q < size) out[q] = static_cast<uint16_t>(c);
+            }
+            cur = nxt;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
+                              int num_sms, cudaStream_t st) {
+    if (num_windows == 0) return cudaSuccess;
+    SweepArgs a{src, n, window, num_windows, cand};
+    const uint32_t smem = kSweepWarpsPerCta * kHashSize * sizeof(uint16_t);
+    cudaError_t e = cudaFuncSetAttribute(cand_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    uint32_t ctas = (num_windows + kSweepWarpsPerCta - 1) / kSweepWarpsPerCta;
+    if (ctas > static_cast<uint32_t>(num_sms)) ctas = num_sms;
+    cand_sweep_kernel<<<ctas, 32 * kSweepWarpsPerCta, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace gcz

@@ -100,6 +100,11 @@ class Context:
     def set_option(self, key, value):
         self._check(L.gcz_set_option(self._h, key.encode(), int(value)))
 
+    def query(self, key):
+        v = ctypes.c_long()
+        self._check(L.gcz_query(self._h, key.encode(), ctypes.byref(v)))
+        return v.value
+
     def sync(self, stream=None):
         self._check(L.gcz_sync(self._h, _stream(stream)))
 

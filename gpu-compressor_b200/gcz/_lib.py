@@ -34,6 +34,7 @@ SIGNATURES = {
     "gcz_version": (_cp, []),
     "gcz_set_option": (_i, [_vp, _cp, _l]),
     "gcz_sync": (_i, [_vp, _vp]),
+    "gcz_query": (_i, [_vp, _cp, ctypes.POINTER(_l)]),
     "gcz_zstd_search_depth_for_level": (_u32, [_u32]),
     "gcz_num_windows": (_sz, [_sz]),
     "gcz_zstd_max_sequences": (_sz, [_sz]),

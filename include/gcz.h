@@ -68,9 +68,16 @@ const char *gcz_last_error(const gcz_ctx *ctx);
 int gcz_device(const gcz_ctx *ctx);
 const char *gcz_version(void);
 
-/* Schedule-only knobs (they never change results): "staged" = 1 stages each
- * window into shared memory with bulk copies (default), 0 reads it through L1. */
+/* Schedule-only knobs (they never change results): "algo" = 2 (default) runs
+ * the candidate sweep then the per-window second stage, 1 the fused
+ * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
+ * memory with bulk copies, 0 reads it through L1; "parse_ctas" = second-stage
+ * CTAs per SM (1-8). */
 int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
+/* Read a knob or a counter: "algo" (1: fused single-warp kernels, 2: candidate
+ * sweep + second stage, the default), "fallback_windows" (Zstd windows whose
+ * speculative parse fell back to the exact warp-wide parse, since creation). */
+int gcz_query(gcz_ctx *ctx, const char *key, long *value);
 
 /* Synchronise `stream` (NULL = the context's stream) and report any error
  * status a kernel enqueued by a _device call recorded since the last check

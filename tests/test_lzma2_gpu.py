@@ -29,16 +29,18 @@ def run_ref_layout(ctx, data, window, max_matches, depth):
             c.cpu().numpy().view(np.uint32)[:B * window])
 
 
-@pytest.mark.parametrize("staged", [1, 0])
+@pytest.mark.parametrize("algo,staged", [(2, 1), (1, 1), (1, 0)], ids=["split", "fused-staged", "fused-l1"])
 @pytest.mark.parametrize("name,spec", cases.CASES, ids=[n for n, _ in cases.CASES])
-def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, staged):
+def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged):
     z, meta = golden
     data = cases.build(spec)
     n = data.size
+    ctx.set_option("algo", algo)
     ctx.set_option("staged", staged)
     try:
         m, c = run_ref_layout(ctx, data, spec["window"], spec["lmax"], spec["ldepth"])
     finally:
+        ctx.set_option("algo", 2)
         ctx.set_option("staged", 1)
     assert int(c.max(initial=0)) <= 1
     assert not np.any(c[n:])

@@ -39,18 +39,20 @@ def run_ref_layout(ctx, data, window, depth, max_seqs):
             sc.cpu().numpy().view(np.uint32)[:B], lc.cpu().numpy().view(np.uint32)[:B])
 
 
-@pytest.mark.parametrize("staged", [1, 0])
+@pytest.mark.parametrize("algo,staged", [(2, 1), (1, 1), (1, 0)], ids=["split", "fused-staged", "fused-l1"])
 @pytest.mark.parametrize("name,spec", cases.CASES, ids=[n for n, _ in cases.CASES])
-def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, staged):
+def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged):
     z, meta = golden
     m = next(x for x in meta if x["name"] == name)
     data = cases.build(spec)
     assert cases.sha(data) == m["input_sha256"]
     W = spec["window"]
+    ctx.set_option("algo", algo)
     ctx.set_option("staged", staged)
     try:
         seqs, lits, sc, lc = run_ref_layout(ctx, data, W, spec["zdepth"], spec["max_seqs"])
     finally:
+        ctx.set_option("algo", 2)
         ctx.set_option("staged", 1)
     np.testing.assert_array_equal(sc, z[f"{name}/zstd_seq_counts"])
     np.testing.assert_array_equal(lc, z[f"{name}/zstd_lit_counts"])
@@ -70,14 +72,20 @@ def test_compact_host_api_matches_oracle(ctx, name, spec):
     np.testing.assert_array_equal(seqs, o_seqs)
 
 
+@pytest.mark.parametrize("algo", [2, 1])
 @pytest.mark.parametrize("seed,n,mix", [(1, 16 << 20, (0.4, 0.4, 0.2)), (31, 5 << 20, (0.05, 0.9, 0.05)),
-                                        (32, 3 << 20 | 12345, (0.9, 0.05, 0.05))])
-def test_synthetic_vs_oracle(ctx, seed, n, mix):
+                                        (32, 3 << 20 | 12345, (0.9, 0.05, 0.05)), (33, 2 << 20, (0.0, 0.0, 1.0)),
+                                        (34, 2 << 20, (0.0, 1.0, 0.0))])
+def test_synthetic_vs_oracle(ctx, seed, n, mix, algo):
     """Zstd L1 plain workload shape (16 MiB, seed 1) and skewed mixes."""
     import gcz
 
     data = gcz.gen_synthetic(seed, n, 8 << 20, mix)
-    seqs, offsets = ctx.zstd_match_find(data, 16)
+    ctx.set_option("algo", algo)
+    try:
+        seqs, offsets = ctx.zstd_match_find(data, 16)
+    finally:
+        ctx.set_option("algo", 2)
     o_seqs, o_off = orc.zstd_sequences(data, 16, threads=16)
     np.testing.assert_array_equal(offsets, o_off)
     np.testing.assert_array_equal(seqs, o_seqs)
