@@ -258,12 +258,18 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
         uint32_t *rm = a.ref_matches ? a.ref_matches + start * a.max_matches * 2u : nullptr;
         uint32_t any = 0;
         const uint32_t nsteps = (size + 31u) >> 5;
+        // The next step's candidates are loaded while this step is verified.
+        uint32_t c_next = (warp < nsteps && warp * 32u + lane + 3u < size) ? cand[warp * 32u + lane] : kNone;
         for (uint32_t st = warp; st < nsteps; st += kL2Threads / 32) {
             const uint32_t q = st * 32u + lane;
             const bool inwin = q < size;
             const bool valid4 = q + 3u < size;
             const uint32_t x = win.u32(q);
-            const uint32_t c = valid4 ? static_cast<uint32_t>(cand[q]) : kNone;
+            const uint32_t c = valid4 ? c_next : kNone;
+            {
+                const uint32_t st2 = st + kL2Threads / 32, q2 = st2 * 32u + lane;
+                c_next = (st2 < nsteps && q2 + 3u < size) ? static_cast<uint32_t>(cand[q2]) : kNone;
+            }
             const bool has = valid4 && a.search_depth > 0 && c != kNone;
             const uint32_t y = has ? win.u32(c) : ~x;
             const bool eq4 = has && y == x;

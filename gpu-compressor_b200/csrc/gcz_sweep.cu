@@ -9,11 +9,15 @@
 // which this kernel computes for every position of every window; the match
 // finders then verify, extend and parse from it.
 //
-// One warp sweeps one window 32 positions per step: __match_any_sync groups
-// the lanes with equal hashes (the in-step predecessor is the next lower lane
-// of the group), the window's table in shared memory supplies the last
-// position of earlier steps, and the highest lane of each group writes it
-// back.  Only the table lives in shared memory (32 KiB), so seven windows are
+// One warp sweeps one window 32 positions per step.  Each lane reads its
+// bucket (the last position of earlier steps), writes its own position and
+// reads it back; when every lane reads back its own position no two lanes of
+// the step share a bucket, the values read are the candidates and the table
+// is up to date.  Otherwise (equal hashes inside a step) the table is restored
+// and __match_any_sync groups the lanes: the in-step predecessor is the next
+// lower lane of the group and the highest lane writes the bucket.  (On this
+// GPU __match_any_sync costs hundreds of cycles, so it is kept off the common
+// path.)  Only the table lives in shared memory (32 KiB), so seven windows are
 // swept per SM; the input streams through coalesced 128-byte loads.
 #include "gcz_common.cuh"
 #include "gcz_kernels.h"
@@ -46,33 +50,73 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
         const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);
         const uint32_t nwords = (size + 3u) >> 2;
         uint16_t *out = a.cand + start;
-        // 128-byte blocks: lane l holds word l; the next block is prefetched.
-        uint32_t cur = lane < nwords ? __ldg(src32 + lane) : 0u;
+        // 128-byte blocks: lane l holds word l.  Two blocks are in flight ahead
+        // of the one being swept, so the load latency stays hidden.
+        uint32_t w0 = lane < nwords ? __ldg(src32 + lane) : 0u;
+        uint32_t w1 = 32u + lane < nwords ? __ldg(src32 + 32u + lane) : 0u;
         for (uint32_t blk = 0; blk * 128u < size; ++blk) {
-            const uint32_t nw = (blk + 1u) * 32u + lane;
-            const uint32_t nxt = nw < nwords ? __ldg(src32 + nw) : 0u;
-            const uint32_t up = __shfl_down_sync(kFull, cur, 1);
-            const uint32_t n0 = __shfl_sync(kFull, nxt, 0);
-            const uint32_t cur1 = lane == 31u ? n0 : up;  // word l+1
+            const uint32_t nw = (blk + 2u) * 32u + lane;
+            const uint32_t w2 = nw < nwords ? __ldg(src32 + nw) : 0u;
+            const uint32_t up = __shfl_down_sync(kFull, w0, 1);
+            const uint32_t n0 = __shfl_sync(kFull, w1, 0);
+            const uint32_t w0n = lane == 31u ? n0 : up;  // word l+1
+            // Hashes of the 4 steps first (independent of the table) ...
+            uint32_t h[4];
+            bool v[4];
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t q = blk * 128u + j * 32u + lane;
                 const uint32_t src_lane = j * 8u + (lane >> 2);
-                const uint32_t lo = __shfl_sync(kFull, cur, src_lane);
-                const uint32_t hi = __shfl_sync(kFull, cur1, src_lane);
-                const uint32_t x = __funnelshift_r(lo, hi, (lane & 3u) * 8u);
-                const bool valid = q + 3u < size;
-                const uint32_t h = hash4(x);
-                const uint32_t g = __match_any_sync(kFull, valid ? h : (0x80000000u | lane));
-                const uint32_t lower = g & lt;
-                const uint32_t tv = valid ? static_cast<uint32_t>(T[h]) : 0xFFFFu;
-                const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv;
+                const uint32_t lo = __shfl_sync(kFull, w0, src_lane);
+                const uint32_t hi = __shfl_sync(kFull, w0n, src_lane);
+                v[j] = q + 3u < size;
+                h[j] = hash4(__funnelshift_r(lo, hi, (lane & 3u) * 8u));
+            }
+            // ... then, step by step: read the bucket, write this position,
+            // read it back.  A lane that does not read back its own position
+            // shares its bucket with another lane of the same step.
+            uint32_t tv[4], dup = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t q = blk * 128u + j * 32u + lane;
+                tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
                 __syncwarp();
-                if (valid && !(g & gt)) T[h] = static_cast<uint16_t>(q);
+                if (v[j]) T[h[j]] = static_cast<uint16_t>(q);
                 __syncwarp();
+                if (v[j] && T[h[j]] != static_cast<uint16_t>(q)) dup |= 1u << j;
+            }
+            uint32_t g[4] = {1u << lane, 1u << lane, 1u << lane, 1u << lane};
+            if (__any_sync(kFull, dup != 0)) {
+                // Rare: some step has equal hashes in two lanes.  Put the table
+                // back as it was before the block (latest steps first, so each
+                // bucket ends with the value its earliest step read) and redo
+                // the block with exact groups.
+                __syncwarp();
+#pragma unroll
+                for (int j = 3; j >= 0; --j) {
+                    if (v[j]) T[h[j]] = static_cast<uint16_t>(tv[j]);
+                    __syncwarp();
+                }
+#pragma unroll
+                for (uint32_t j = 0; j < 4; ++j) {
+                    const uint32_t q = blk * 128u + j * 32u + lane;
+                    g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+                    tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
+                    __syncwarp();
+                    if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
+                    __syncwarp();
+                }
+            }
+            // ... then the candidates.
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t q = blk * 128u + j * 32u + lane;
+                const uint32_t lower = g[j] & lt;
+                const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv[j];
                 if (q < size) out[q] = static_cast<uint16_t>(c);
             }
-            cur = nxt;
+            w0 = w1;
+            w1 = w2;
         }
         __syncwarp();
     }

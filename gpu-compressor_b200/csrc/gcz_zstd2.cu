@@ -96,17 +96,33 @@ struct Win {
     }
 };
 
-// 4 bits: byte k of (a ^ b) is zero.
-__device__ __forceinline__ uint32_t eq_nibble(uint32_t a, uint32_t b) {
-    const uint32_t x = a ^ b;
-    const uint32_t y = ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
-    return (y * 0x00204081u) >> 28;
-}
+// Aligned word stream over the staged window: next() returns the 4 bytes at
+// the current position and advances by 4, with one shared-memory load and one
+// funnel shift per call.
+struct Stream {
+    const uint32_t *w;
+    uint32_t j, sh, cur;
+    __device__ __forceinline__ Stream(const Win &win, int pos) {
+        w = reinterpret_cast<const uint32_t *>(win.d - kPre);
+        const uint32_t a = static_cast<uint32_t>(pos + static_cast<int>(kPre));
+        j = a >> 2;
+        sh = (a & 3u) * 8u;
+        cur = w[j];
+    }
+    __device__ __forceinline__ uint32_t next() {
+        const uint32_t nx = w[++j];
+        const uint32_t v = __funnelshift_r(cur, nx, sh);
+        cur = nx;
+        return v;
+    }
+};
 
-// First index in [len, lim) where bytes c+i and q+i differ, else lim.
-__device__ __forceinline__ uint32_t extend(const Win &w, uint32_t c, uint32_t q, uint32_t len, uint32_t lim) {
+// First index in [0, lim) where bytes c+i and q+i differ, else lim.
+__device__ __forceinline__ uint32_t extend(const Win &win, uint32_t c, uint32_t q, uint32_t lim) {
+    Stream sc(win, static_cast<int>(c)), sq(win, static_cast<int>(q));
+    uint32_t len = 0;
     while (len < lim) {
-        const uint32_t d = w.u32(static_cast<int>(q + len)) ^ w.u32(static_cast<int>(c + len));
+        const uint32_t d = sq.next() ^ sc.next();
         if (d) {
             len += (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3;
             return len < lim ? len : lim;
@@ -120,22 +136,69 @@ __device__ __forceinline__ bool eq3(const Win &w, uint32_t a, uint32_t b) {
     return ((w.u32(static_cast<int>(a)) ^ w.u32(static_cast<int>(b))) & 0xFFFFFFu) == 0u;
 }
 
-// Bits i < n (n <= 32) where the 3 bytes at p+i equal those at p+i-d and d <= p+i.
-// A[k] = bytes p+4k .. p+4k+3.
-__device__ __forceinline__ uint32_t rep_bits(const Win &w, const uint32_t (&A)[9], uint32_t p, uint32_t d,
-                                             uint32_t n) {
-    if (n == 0 || d > p + n) return 0u;
-    const int base = static_cast<int>(p) - static_cast<int>(d);
-    const uint32_t words = (n + 2u + 3u) >> 2;  // bytes [0, n+2)
-    uint64_t eq = 0;
-#pragma unroll
-    for (uint32_t k = 0; k < 9; ++k) {
-        if (k < words) eq |= static_cast<uint64_t>(eq_nibble(A[k], w.u32(base + 4 * static_cast<int>(k)))) << (4 * k);
+// 0x80 in every byte of x that is zero.
+__device__ __forceinline__ uint32_t zero_bytes(uint32_t x) {
+    return ~(((x & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | x) & 0x80808080u;
+}
+
+// Positions k+j (j < 4) of a 4-position chunk where offset d is usable
+// (d <= p+k+j), as byte lanes: 0xFF per usable position.
+__device__ __forceinline__ uint32_t usable(uint32_t d, uint32_t p, uint32_t k) {
+    if (d <= p + k) return 0xFFFFFFFFu;
+    const uint32_t v = d - p - k;  // first usable j
+    return v >= 4u ? 0u : (0xFFFFFFFFu << (8u * v));
+}
+
+// Bit 8j+7: the 3 bytes at chunk position j are all zero in the xor stream
+// whose zero-byte masks are z (this word) and y (next word).
+__device__ __forceinline__ uint32_t three_equal(uint32_t z, uint32_t y) {
+    return z & __funnelshift_r(z, y, 8) & __funnelshift_r(z, y, 16);
+}
+
+// First offset i in [0, n) (n <= 32) at which one of the repeat offsets d
+// (d <= p+i) gives 3 equal bytes (src[p+i..p+i+2] == src[p+i-d..]), else n.
+// Positions are examined 4 at a time and the search stops at the first hit.
+__device__ __forceinline__ uint32_t rep_search(const Win &win, uint32_t p, uint32_t n, uint32_t r0, uint32_t r1,
+                                               uint32_t r2) {
+    if (n == 0) return 0;
+    // offsets usable somewhere in [p, p+n), duplicates dropped
+    const bool e0 = r0 < p + n;
+    const bool e1 = r1 < p + n && r1 != r0;
+    const bool e2 = r2 < p + n && r2 != r0 && r2 != r1;
+    if (!(e0 || e1 || e2)) return n;
+    Stream a(win, static_cast<int>(p));
+    Stream b0(win, e0 ? static_cast<int>(p) - static_cast<int>(r0) : 0);
+    Stream b1(win, e1 ? static_cast<int>(p) - static_cast<int>(r1) : 0);
+    Stream b2(win, e2 ? static_cast<int>(p) - static_cast<int>(r2) : 0);
+    const uint32_t A = a.next();
+    uint32_t z0 = e0 ? zero_bytes(A ^ b0.next()) : 0u;
+    uint32_t z1 = e1 ? zero_bytes(A ^ b1.next()) : 0u;
+    uint32_t z2 = e2 ? zero_bytes(A ^ b2.next()) : 0u;
+    uint32_t found = n;
+    for (uint32_t k = 0; k < found; k += 4u) {
+        const uint32_t A1 = a.next();
+        uint32_t t = 0;
+        if (e0) {
+            const uint32_t y = zero_bytes(A1 ^ b0.next());
+            t |= three_equal(z0, y) & usable(r0, p, k);
+            z0 = y;
+        }
+        if (e1) {
+            const uint32_t y = zero_bytes(A1 ^ b1.next());
+            t |= three_equal(z1, y) & usable(r1, p, k);
+            z1 = y;
+        }
+        if (e2) {
+            const uint32_t y = zero_bytes(A1 ^ b2.next());
+            t |= three_equal(z2, y) & usable(r2, p, k);
+            z2 = y;
+        }
+        if (t) {
+            const uint32_t i = k + ((static_cast<uint32_t>(__ffs(t)) - 1u) >> 3);
+            if (i < found) found = i;
+        }
     }
-    uint64_t m = eq & (eq >> 1) & (eq >> 2);
-    if (d > p) m &= ~((1ull << (d - p)) - 1ull);
-    const uint32_t lo = static_cast<uint32_t>(m);
-    return n >= 32 ? lo : (lo & ((1u << n) - 1u));
+    return found;
 }
 
 struct PState {
@@ -169,46 +232,35 @@ __device__ __forceinline__ bool parse_step(const Win &w, const uint32_t *bm, con
         f = p;
         hash = true;
     } else {
-        uint32_t n = H ? static_cast<uint32_t>(__ffs(H)) - 1u : nscan;
-        uint32_t A[9];
-#pragma unroll
-        for (uint32_t k = 0; k < 9; ++k) A[k] = w.u32(static_cast<int>(p + 4u * k));
-        // Shrink the range after each repeat offset: only the first event matters.
-        uint32_t R = rep_bits(w, A, p, s.r0, n);
-        if (R) n = static_cast<uint32_t>(__ffs(R)) - 1u;
-        if (s.r1 != s.r0) {
-            const uint32_t R1 = rep_bits(w, A, p, s.r1, n);
-            if (R1) {
-                R |= R1;
-                n = static_cast<uint32_t>(__ffs(R1)) - 1u;
-            }
-        }
-        if (s.r2 != s.r0 && s.r2 != s.r1) R |= rep_bits(w, A, p, s.r2, n);
-        if (R) {
-            f = p + static_cast<uint32_t>(__ffs(R)) - 1u;
+        const uint32_t n = H ? static_cast<uint32_t>(__ffs(H)) - 1u : nscan;  // positions without a hash match
+        const uint32_t r = rep_search(w, p, n, s.r0, s.r1, s.r2);
+        if (r < n) {
+            f = p + r;
             hash = false;
         } else if (H) {
-            f = p + (static_cast<uint32_t>(__ffs(H)) - 1u);
+            f = p + n;
             hash = true;
         } else {
             s.p = p + nscan;
             return false;
         }
     }
+    // Both candidates (f and f+1, for the lazy step) are loaded together.
+    const uint32_t cf = cand_at(cand, f), cf1 = cand_at(cand, f + 1u);
     if (hash) {
-        const uint32_t c = cand_at(cand, f);
+        const uint32_t c = cf;
         off = f - c;
-        len = extend(w, c + kMinMatch, f + kMinMatch, 0u, size - f - kMinMatch) + kMinMatch;
+        len = extend(w, c + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
     } else {  // first repeat offset with 3 equal bytes wins (:259-275)
         if (s.r0 <= f && eq3(w, f, f - s.r0)) off = s.r0;
         else if (s.r1 <= f && eq3(w, f, f - s.r1)) off = s.r1;
         else off = s.r2;
-        len = extend(w, f - off + kMinMatch, f + kMinMatch, 0u, size - f - kMinMatch) + kMinMatch;
+        len = extend(w, f - off + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
     }
     if (lazy && f + 4u < size && bm_bit(bm, f + 1u)) {  // :278-307
-        const uint32_t c1 = cand_at(cand, f + 1u);
+        const uint32_t c1 = cf1;
         const uint32_t len2 =
-            extend(w, c1 + kMinMatch, f + 1u + kMinMatch, 0u, size - f - 1u - kMinMatch) + kMinMatch;
+            extend(w, c1 + kMinMatch, f + 1u + kMinMatch, size - f - 1u - kMinMatch) + kMinMatch;
         if (len2 > len + 1u) {
             f += 1u;
             len = len2;
@@ -269,16 +321,16 @@ __device__ void warp_parse(const Win &w, const uint32_t *bm, const uint16_t *can
         if ((hb >> f0) & 1u) {
             const uint32_t c = cand_at(cand, f);
             off = f - c;
-            len = extend(w, c + kMinMatch, f + kMinMatch, 0u, size - f - kMinMatch) + kMinMatch;
+            len = extend(w, c + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
         } else {
             const uint32_t r = __shfl_sync(kFull, rsel, f0);
             off = r == 0u ? r0 : (r == 1u ? r1 : r2);
-            len = extend(w, f - off + kMinMatch, f + kMinMatch, 0u, size - f - kMinMatch) + kMinMatch;
+            len = extend(w, f - off + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
         }
         if (lazy && f + 4u < size && bm_bit(bm, f + 1u)) {
             const uint32_t c1 = cand_at(cand, f + 1u);
             const uint32_t len2 =
-                extend(w, c1 + kMinMatch, f + 1u + kMinMatch, 0u, size - f - 1u - kMinMatch) + kMinMatch;
+                extend(w, c1 + kMinMatch, f + 1u + kMinMatch, size - f - 1u - kMinMatch) + kMinMatch;
             if (len2 > len + 1u) {
                 f += 1u;
                 len = len2;
@@ -329,15 +381,25 @@ __global__ void __launch_bounds__(kThreads) zstd_parse_kernel(Zstd2Args a) {
         __syncthreads();
         if (S.flags & 2u) return;  // bulk copy never completed: status already recorded, all threads leave
         const uint32_t nsteps = (size + 31u) >> 5;
-        for (uint32_t st = warp; st < kBmWords; st += kThreads / 32) {
-            const uint32_t q = st * 32u + lane;
-            bool hm = false;
-            if (st < nsteps && q + 3u < size && q > 0u) {
-                const uint32_t c = cand_at(cand, q);
-                hm = eq3(win, q, c);
+        // Batches of kVB steps per warp: all kVB candidate loads are issued
+        // before any is used, so one memory latency covers the batch.
+        constexpr uint32_t kVB = 16;
+        for (uint32_t b0 = warp * kVB; b0 < kBmWords; b0 += (kThreads / 32) * kVB) {
+            uint32_t cv[kVB];
+#pragma unroll
+            for (uint32_t u = 0; u < kVB; ++u) {
+                const uint32_t q = (b0 + u) * 32u + lane;
+                cv[u] = (b0 + u < nsteps && q + 3u < size && q > 0u) ? static_cast<uint32_t>(cand[q]) : 0x10000u;
             }
-            const uint32_t bits = __ballot_sync(kFull, hm);
-            if (lane == 0) S.bm[st] = bits;
+#pragma unroll
+            for (uint32_t u = 0; u < kVB; ++u) {
+                const uint32_t st = b0 + u;
+                const uint32_t q = st * 32u + lane;
+                bool hm = false;
+                if (cv[u] != 0x10000u) hm = eq3(win, q, cv[u] == 0xFFFFu ? 0u : cv[u]);
+                const uint32_t bits = __ballot_sync(kFull, hm);
+                if (lane == 0 && st < kBmWords) S.bm[st] = bits;
+            }
         }
         __syncthreads();
 
