@@ -15,9 +15,6 @@ namespace {
 
 constexpr uint32_t kW = GCZ_WINDOW;
 constexpr uint32_t kMaxSeqs = GCZ_ZSTD_MAX_SEQ_PER_WINDOW;  // chunk_size / 3
-// Host-buffer calls process the input in slices of this many windows so that
-// device memory stays bounded (and copies of one slice overlap another).
-constexpr uint32_t kSliceWindows = 2048;  // 128 MiB of input
 
 struct DevBuf {
     void *p = nullptr;
@@ -32,6 +29,23 @@ struct EventPair {
     cudaEvent_t a = nullptr, b = nullptr;
 };
 
+// Device scratch of one match-find step.
+struct Scratch {
+    DevBuf packed, counts, cand, seg;
+};
+
+// One stage of the host-buffer pipeline: its own stream, input, scratch and
+// outputs, so that the copies of one slice overlap the kernels of another.
+struct Slot {
+    Scratch sc;
+    DevBuf in, offsets, seqs, lz_packed, lz_has;
+    HostBuf h_off, h_packed;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+    size_t b0 = 0, sb = 0, off = 0, len = 0;
+};
+
 }  // namespace
 
 struct gcz_ctx {
@@ -41,8 +55,9 @@ struct gcz_ctx {
     std::mutex mu;
     std::string err;
     uint32_t *d_status = nullptr;
-    DevBuf in, packed, counts, offsets, seqs, lz_packed, lz_has, cand, seg;
-    HostBuf h_offsets, h_packed;
+    Scratch sc;      // scratch of the _device entry points
+    Slot slots[2];   // host-buffer pipeline
+    uint32_t slice_windows = 1024;  // windows per pipeline slice (64 MiB)
     int staged = 1;
     int algo = 2;          // 1: fused single-warp kernels, 2: candidate sweep + second stage
     int parse_ctas = 3;    // second-stage CTAs per SM
@@ -156,21 +171,21 @@ size_t nwin(size_t n) { return (n + kW - 1) / kW; }
 
 // Zstd on device memory for one contiguous range of windows: packed sequences
 // into ctx scratch, counts, offsets (num+1, relative), compact expansion.
-int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth, void *d_seqs, uint64_t capacity,
-                     uint64_t *d_offsets, cudaStream_t st) {
+int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, uint32_t depth, void *d_seqs,
+                     uint64_t capacity, uint64_t *d_offsets, cudaStream_t st) {
     const size_t nb = nwin(n);
     int r;
-    if ((r = ensure_dev(c, c->packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
-    if ((r = ensure_dev(c, c->counts, nb * 4)) != GCZ_OK) return r;
-    uint32_t *counts = static_cast<uint32_t *>(c->counts.p);
+    if ((r = ensure_dev(c, sc.packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sc.counts, nb * 4)) != GCZ_OK) return r;
+    uint32_t *counts = static_cast<uint32_t *>(sc.counts.p);
     if (c->algo == 2) {
-        if ((r = ensure_dev(c, c->cand, n * 2 + 64)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, c->seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sc.cand, n * 2 + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sc.seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
     }
     // The profiled interval covers the whole match-find step (all its kernels).
     ProfScope ps(c, st);
     if (c->algo == 2) {
-        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st));
         gcz::Zstd2Launch l{};
         l.src = d_src;
@@ -180,8 +195,8 @@ int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
         l.num_windows = (uint32_t)nb;
         l.search_depth = depth;
         l.max_seqs = kMaxSeqs;
-        l.seg = c->seg.p;
-        l.packed = c->packed.p;
+        l.seg = sc.seg.p;
+        l.packed = sc.packed.p;
         l.seq_counts = counts;
         l.status = c->d_status;
         l.num_sms = c->num_sms;
@@ -196,7 +211,7 @@ int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
         l.num_windows = (uint32_t)nb;
         l.search_depth = depth;
         l.max_seqs = kMaxSeqs;
-        l.packed = c->packed.p;
+        l.packed = sc.packed.p;
         l.seq_counts = counts;
         l.status = c->d_status;
         l.num_sms = c->num_sms;
@@ -205,18 +220,18 @@ int zstd_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
         c->all_launches += 1;
     }
     GCZ_CUDA(c, gcz::launch_scan_counts(counts, (uint32_t)nb, d_offsets, st));
-    GCZ_CUDA(c, gcz::launch_expand_seqs(c->packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
+    GCZ_CUDA(c, gcz::launch_expand_seqs(sc.packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
                                         c->d_status, c->num_sms, st));
     c->all_launches += 2;
     return GCZ_OK;
 }
 
-int lzma_run(gcz_ctx *c, const gcz::LzmaLaunch &l, cudaStream_t st) {
+int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st) {
     int r;
+    if (c->algo == 2 && (r = ensure_dev(c, sc.cand, l.n * 2 + 64)) != GCZ_OK) return r;
     ProfScope ps(c, st);
     if (c->algo == 2) {
-        if ((r = ensure_dev(c, c->cand, l.n * 2 + 64)) != GCZ_OK) return r;
-        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st));
         GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, st));
         c->all_launches += 2;
@@ -227,8 +242,8 @@ int lzma_run(gcz_ctx *c, const gcz::LzmaLaunch &l, cudaStream_t st) {
     return GCZ_OK;
 }
 
-int lzma_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth, uint32_t *d_packed, uint8_t *d_has,
-                     cudaStream_t st) {
+int lzma_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, uint32_t depth, uint32_t *d_packed,
+                     uint8_t *d_has, cudaStream_t st) {
     const size_t nb = nwin(n);
     gcz::LzmaLaunch l{};
     l.src = d_src;
@@ -242,7 +257,7 @@ int lzma_device_core(gcz_ctx *c, const uint8_t *d_src, size_t n, uint32_t depth,
     l.status = c->d_status;
     l.num_sms = c->num_sms;
     l.staged = c->staged;
-    return lzma_run(c, l, st);
+    return lzma_run(c, sc, l, st);
 }
 
 bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
@@ -268,8 +283,12 @@ extern "C" int gcz_create(int device_id, gcz_ctx **out) {
         return GCZ_ECUDA;
     }
     c->num_sms = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&c->d_status, 16) != cudaSuccess || cudaMemset(c->d_status, 0, 16) != cudaSuccess) {
+    bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMalloc(&c->d_status, 16) == cudaSuccess && cudaMemset(c->d_status, 0, 16) == cudaSuccess;
+    for (Slot &sl : c->slots)
+        ok = ok && cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
         cudaGetLastError();
         if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
@@ -284,11 +303,21 @@ extern "C" void gcz_destroy(gcz_ctx *c) {
     {
         DeviceGuard g(c->device);
         cudaStreamSynchronize(c->stream);
-        for (DevBuf *b : {&c->in, &c->packed, &c->counts, &c->offsets, &c->seqs, &c->lz_packed, &c->lz_has, &c->cand,
-                          &c->seg})
-            if (b->p) cudaFree(b->p);
-        for (HostBuf *b : {&c->h_offsets, &c->h_packed})
-            if (b->p) cudaFreeHost(b->p);
+        auto free_scratch = [](Scratch &x) {
+            for (DevBuf *b : {&x.packed, &x.counts, &x.cand, &x.seg})
+                if (b->p) cudaFree(b->p);
+        };
+        free_scratch(c->sc);
+        for (Slot &sl : c->slots) {
+            if (sl.st) cudaStreamSynchronize(sl.st);
+            free_scratch(sl.sc);
+            for (DevBuf *b : {&sl.in, &sl.offsets, &sl.seqs, &sl.lz_packed, &sl.lz_has})
+                if (b->p) cudaFree(b->p);
+            for (HostBuf *b : {&sl.h_off, &sl.h_packed})
+                if (b->p) cudaFreeHost(b->p);
+            if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.st) cudaStreamDestroy(sl.st);
+        }
         for (auto &e : c->events) {
             cudaEventDestroy(e.a);
             cudaEventDestroy(e.b);
@@ -312,6 +341,10 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
     }
     if (!strcmp(key, "algo") && (value == 1 || value == 2)) {
         c->algo = (int)value;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "slice_windows") && value >= 1 && value <= (1L << 20)) {
+        c->slice_windows = (uint32_t)value;
         return GCZ_OK;
     }
     if (!strcmp(key, "parse_ctas") && value >= 1 && value <= 8) {
@@ -375,46 +408,72 @@ extern "C" int gcz_zstd_match_find_device(gcz_ctx *c, const uint8_t *d_src, size
         GCZ_CUDA(c, cudaMemsetAsync(d_offsets, 0, 8, st));
         return GCZ_OK;
     }
-    return zstd_device_core(c, d_src, n, search_depth, d_seqs, seq_capacity, d_offsets, st);
+    return zstd_device_core(c, c->sc, d_src, n, search_depth, d_seqs, seq_capacity, d_offsets, st);
 }
 
+namespace {
+// Second half of a Zstd pipeline slice: wait for its offsets, then queue the
+// copy of its sequences into the caller's array.
+int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, uint64_t *offsets, uint64_t &done) {
+    GCZ_CUDA(c, cudaEventSynchronize(sl.ev));
+    const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);
+    const uint64_t total = ho[sl.sb];
+    sl.busy = false;
+    if (done + total > cap)
+        return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)(done + total), cap);
+    if (total) GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, sl.seqs.p, total * 16, cudaMemcpyDeviceToHost, sl.st));
+    for (size_t i = 1; i <= sl.sb; i++) offsets[sl.b0 + i] = done + ho[i];
+    done += total;
+    return GCZ_OK;
+}
+
+int drain_slots(gcz_ctx *c) {
+    for (Slot &sl : c->slots) GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+    return read_status(c, c->stream);
+}
+}  // namespace
+
+// Slices of slice_windows windows alternate between two slots (streams): the
+// H2D copy and kernels of slice k run while slice k-1's sequences are copied
+// back.
 extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
                                    gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets) {
     if (!c) return GCZ_EINVAL;
     std::lock_guard<std::mutex> lk(c->mu);
     if ((n && (!src || !seqs)) || !offsets) return fail(c, GCZ_EINVAL, "null pointer");
     DeviceGuard g(c->device);
-    cudaStream_t st = c->stream;
     const size_t nb = nwin(n);
     offsets[0] = 0;
-    int r;
-    uint64_t done = 0;  // sequences written so far
-    for (size_t b0 = 0; b0 < nb; b0 += kSliceWindows) {
-        const size_t b1 = std::min(nb, b0 + (size_t)kSliceWindows), sb = b1 - b0;
-        const size_t off = b0 * (size_t)kW, len = std::min(n - off, sb * (size_t)kW);
-        if ((r = ensure_dev(c, c->in, sb * (size_t)kW + 64)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, c->offsets, (sb + 1) * 8)) != GCZ_OK) return r;
-        const size_t slice_cap = gcz_zstd_max_sequences(len);
-        if ((r = ensure_dev(c, c->seqs, std::max<size_t>(slice_cap, 1) * 16)) != GCZ_OK) return r;
-        if ((r = ensure_host(c, c->h_offsets, (sb + 1) * 8)) != GCZ_OK) return r;
-        GCZ_CUDA(c, cudaMemcpyAsync(c->in.p, src + off, len, cudaMemcpyHostToDevice, st));
-        if ((r = zstd_device_core(c, static_cast<const uint8_t *>(c->in.p), len, search_depth, c->seqs.p, slice_cap,
-                                  static_cast<uint64_t *>(c->offsets.p), st)) != GCZ_OK)
-            return r;
-        uint64_t *ho = static_cast<uint64_t *>(c->h_offsets.p);
-        GCZ_CUDA(c, cudaMemcpyAsync(ho, c->offsets.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, st));
-        if ((r = read_status(c, st)) != GCZ_OK) return r;
-        const uint64_t total = ho[sb];
-        if (done + total > seq_capacity)
-            return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)(done + total),
-                        seq_capacity);
-        if (total)
-            GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, c->seqs.p, total * 16, cudaMemcpyDeviceToHost, st));
-        for (size_t i = 1; i <= sb; i++) offsets[b0 + i] = done + ho[i];
-        done += total;
-        GCZ_CUDA(c, cudaStreamSynchronize(st));
+    int r = GCZ_OK;
+    uint64_t done = 0;  // sequences copied so far
+    size_t k = 0;
+    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+        Slot &sl = c->slots[k & 1];
+        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sl.b0 = b0;
+        sl.sb = sb;
+        sl.off = b0 * (size_t)kW;
+        sl.len = std::min(n - sl.off, sb * (size_t)kW);
+        const size_t slice_cap = gcz_zstd_max_sequences(sl.len);
+        if ((r = ensure_dev(c, sl.in, sb * (size_t)kW + 64)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.offsets, (sb + 1) * 8)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(slice_cap, 1) * 16)) != GCZ_OK) break;
+        if ((r = ensure_host(c, sl.h_off, (sb + 1) * 8)) != GCZ_OK) break;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.in.p, src + sl.off, sl.len, cudaMemcpyHostToDevice, sl.st));
+        if ((r = zstd_device_core(c, sl.sc, static_cast<const uint8_t *>(sl.in.p), sl.len, search_depth, sl.seqs.p,
+                                  slice_cap, static_cast<uint64_t *>(sl.offsets.p), sl.st)) != GCZ_OK)
+            break;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+        GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
+        sl.busy = true;
+        Slot &prev = c->slots[(k + 1) & 1];
+        if (prev.busy) r = zstd_finish_slot(c, prev, seqs, seq_capacity, offsets, done);
     }
-    return GCZ_OK;
+    Slot &last = c->slots[(k + 1) & 1];
+    if (r == GCZ_OK && last.busy) r = zstd_finish_slot(c, last, seqs, seq_capacity, offsets, done);
+    for (Slot &sl : c->slots) sl.busy = false;
+    const int r2 = drain_slots(c);
+    return r != GCZ_OK ? r : r2;
 }
 
 extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *d_input, uint32_t *d_sequences,
@@ -436,10 +495,10 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
     uint64_t n_eff = std::min<uint64_t>(total_input_size, nb * chunk_size);
     if (c->algo == 2) {
         int r;
-        if ((r = ensure_dev(c, c->cand, n_eff * 2 + 64)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, c->seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->sc.cand, n_eff * 2 + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, c->sc.seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
         ProfScope ps(c, st);
-        uint16_t *cand = static_cast<uint16_t *>(c->cand.p);
+        uint16_t *cand = static_cast<uint16_t *>(c->sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(d_input, n_eff, chunk_size, (uint32_t)nb, cand, c->num_sms, st));
         gcz::Zstd2Launch l{};
         l.src = d_input;
@@ -449,7 +508,7 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
         l.num_windows = (uint32_t)nb;
         l.search_depth = search_depth;
         l.max_seqs = max_sequences_per_chunk;
-        l.seg = c->seg.p;
+        l.seg = c->sc.seg.p;
         l.ref_seqs = d_sequences;
         l.seq_counts = d_seq_counts;
         l.lit_counts = d_lit_counts;
@@ -495,39 +554,57 @@ extern "C" int gcz_lzma2_match_find_device(gcz_ctx *c, const uint8_t *d_src, siz
     if (nwin(n) > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "input too large");
     DeviceGuard g(c->device);
     if (n == 0) return GCZ_OK;
-    return lzma_device_core(c, d_src, n, search_depth, d_packed, d_has_matches, pick_stream(c, stream));
+    return lzma_device_core(c, c->sc, d_src, n, search_depth, d_packed, d_has_matches, pick_stream(c, stream));
 }
 
 namespace {
-// Host-side slices for the two LZMA2 host entry points.
+// Host-side slices for the two LZMA2 host entry points, alternating between
+// the two pipeline slots; `consume` sees each slice's packed results on the
+// host once they have arrived.
 template <class Consume>
 int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, uint32_t *packed_out,
                      uint8_t *has_out, Consume consume) {
-    cudaStream_t st = c->stream;
     const size_t nb = nwin(n);
-    int r;
-    for (size_t b0 = 0; b0 < nb; b0 += kSliceWindows) {
-        const size_t b1 = std::min(nb, b0 + (size_t)kSliceWindows), sb = b1 - b0;
-        const size_t off = b0 * (size_t)kW, len = std::min(n - off, sb * (size_t)kW);
-        if ((r = ensure_dev(c, c->in, sb * (size_t)kW + 64)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, c->lz_packed, sb * (size_t)kW * 4)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, c->lz_has, sb + 16)) != GCZ_OK) return r;
-        GCZ_CUDA(c, cudaMemcpyAsync(c->in.p, src + off, len, cudaMemcpyHostToDevice, st));
-        if ((r = lzma_device_core(c, static_cast<const uint8_t *>(c->in.p), len, depth,
-                                  static_cast<uint32_t *>(c->lz_packed.p), static_cast<uint8_t *>(c->lz_has.p), st)) !=
-            GCZ_OK)
-            return r;
-        uint32_t *dst = packed_out ? packed_out + off : nullptr;
+    int r = GCZ_OK;
+    auto finish = [&](Slot &sl) -> int {
+        GCZ_CUDA(c, cudaEventSynchronize(sl.ev));
+        sl.busy = false;
+        consume(sl.off, sl.len, packed_out ? packed_out + sl.off : static_cast<const uint32_t *>(sl.h_packed.p));
+        return GCZ_OK;
+    };
+    size_t k = 0;
+    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+        Slot &sl = c->slots[k & 1];
+        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sl.b0 = b0;
+        sl.sb = sb;
+        sl.off = b0 * (size_t)kW;
+        sl.len = std::min(n - sl.off, sb * (size_t)kW);
+        if ((r = ensure_dev(c, sl.in, sb * (size_t)kW + 64)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.lz_packed, sb * (size_t)kW * 4)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.lz_has, sb + 16)) != GCZ_OK) break;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.in.p, src + sl.off, sl.len, cudaMemcpyHostToDevice, sl.st));
+        if ((r = lzma_device_core(c, sl.sc, static_cast<const uint8_t *>(sl.in.p), sl.len, depth,
+                                  static_cast<uint32_t *>(sl.lz_packed.p), static_cast<uint8_t *>(sl.lz_has.p),
+                                  sl.st)) != GCZ_OK)
+            break;
+        uint32_t *dst = packed_out ? packed_out + sl.off : nullptr;
         if (!dst) {
-            if ((r = ensure_host(c, c->h_packed, sb * (size_t)kW * 4)) != GCZ_OK) return r;
-            dst = static_cast<uint32_t *>(c->h_packed.p);
+            if ((r = ensure_host(c, sl.h_packed, sb * (size_t)kW * 4)) != GCZ_OK) break;
+            dst = static_cast<uint32_t *>(sl.h_packed.p);
         }
-        GCZ_CUDA(c, cudaMemcpyAsync(dst, c->lz_packed.p, len * 4, cudaMemcpyDeviceToHost, st));
-        if (has_out) GCZ_CUDA(c, cudaMemcpyAsync(has_out + b0, c->lz_has.p, sb, cudaMemcpyDeviceToHost, st));
-        if ((r = read_status(c, st)) != GCZ_OK) return r;
-        consume(off, len, dst);
+        GCZ_CUDA(c, cudaMemcpyAsync(dst, sl.lz_packed.p, sl.len * 4, cudaMemcpyDeviceToHost, sl.st));
+        if (has_out) GCZ_CUDA(c, cudaMemcpyAsync(has_out + b0, sl.lz_has.p, sb, cudaMemcpyDeviceToHost, sl.st));
+        GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
+        sl.busy = true;
+        Slot &prev = c->slots[(k + 1) & 1];
+        if (prev.busy) r = finish(prev);
     }
-    return GCZ_OK;
+    Slot &last = c->slots[(k + 1) & 1];
+    if (r == GCZ_OK && last.busy) r = finish(last);
+    for (Slot &sl : c->slots) sl.busy = false;
+    const int r2 = drain_slots(c);
+    return r != GCZ_OK ? r : r2;
 }
 }  // namespace
 
@@ -604,7 +681,7 @@ extern "C" int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *c, const uint8_t 
     l.status = c->d_status;
     l.num_sms = c->num_sms;
     l.staged = c->staged;
-    return lzma_run(c, l, st);
+    return lzma_run(c, c->sc, l, st);
 }
 
 // =========================================================================== profiling

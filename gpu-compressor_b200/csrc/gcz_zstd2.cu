@@ -122,6 +122,82 @@ __device__ __forceinline__ uint32_t extend_warp(const Win &w, uint32_t c, uint32
     }
 }
 
+// Two extensions at once: lanes 0-15 extend (ca, qa) up to la, lanes 16-31
+// extend (cb, qb) up to lb, 64 bytes per half per iteration.
+__device__ __forceinline__ void extend_pair(const Win &w, uint32_t ca, uint32_t qa, uint32_t la, uint32_t cb,
+                                            uint32_t qb, uint32_t lb, uint32_t &ra, uint32_t &rb) {
+    const uint32_t lane = lane_id(), half = lane >> 4, hl = lane & 15u;
+    const uint32_t c = half ? cb : ca, q = half ? qb : qa, lim = half ? lb : la;
+    bool da = false, db = false;
+    ra = 0;
+    rb = 0;
+    for (uint32_t len = 0;; len += 64u) {
+        const uint32_t k = len + 4u * hl;
+        uint32_t res = k;
+        if (k < lim) {
+            const uint32_t d = w.u32(static_cast<int>(q + k)) ^ w.u32(static_cast<int>(c + k));
+            const uint32_t fb = d ? (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3 : 4u;
+            const uint32_t rem = lim - k;
+            res = k + (fb < rem ? fb : rem);
+        }
+        const uint32_t sb = __ballot_sync(kFull, res < k + 4u);
+        const uint32_t sa = sb & 0xFFFFu, sbb = sb >> 16;
+        const uint32_t va = __shfl_sync(kFull, res, sa ? __ffs(sa) - 1 : 0);
+        const uint32_t vb = __shfl_sync(kFull, res, sbb ? 16 + __ffs(sbb) - 1 : 16);
+        if (!da && sa) {
+            ra = va;
+            da = true;
+        }
+        if (!db && sbb) {
+            rb = vb;
+            db = true;
+        }
+        if (da && db) return;
+    }
+}
+
+// Rolling register buffer of candidates for one warp: lane l holds
+// cand[base + l], cand[base + 32 + l] and cand[base + 64 + l] (the third block
+// is a prefetch), base 32-aligned.
+struct CandBuf {
+    const uint16_t *cand;
+    uint32_t size, base, c0, c1, c2;
+    __device__ __forceinline__ uint32_t ld(uint32_t pos) const {
+        return pos < size ? static_cast<uint32_t>(cand[pos]) : 0u;
+    }
+    __device__ __forceinline__ void init(uint32_t p) {
+        const uint32_t lane = lane_id();
+        base = p & ~31u;
+        c0 = ld(base + lane);
+        c1 = ld(base + 32u + lane);
+        c2 = ld(base + 64u + lane);
+    }
+    // Make positions [p, p+33) available (p uniform).
+    __device__ __forceinline__ void advance(uint32_t p) {
+        const uint32_t nb = p & ~31u, lane = lane_id();
+        if (nb == base) return;
+        if (nb == base + 32u) {
+            c0 = c1;
+            c1 = c2;
+            c2 = ld(nb + 64u + lane);
+        } else if (nb == base + 64u) {
+            c0 = c2;
+            c1 = ld(nb + 32u + lane);
+            c2 = ld(nb + 64u + lane);
+        } else {
+            init(p);
+            return;
+        }
+        base = nb;
+    }
+    // cand[pos] for pos in [base, base+96) (pos uniform).
+    __device__ __forceinline__ uint32_t get(uint32_t pos) const {
+        const uint32_t k = pos - base;
+        const uint32_t r = k < 32u ? c0 : (k < 64u ? c1 : c2);
+        return __shfl_sync(kFull, r, k & 31u);
+    }
+};
+
 __device__ __forceinline__ bool eq3(const Win &w, uint32_t a, uint32_t b) {
     return ((w.u32(static_cast<int>(a)) ^ w.u32(static_cast<int>(b))) & 0xFFFFFFu) == 0u;
 }
@@ -141,8 +217,8 @@ struct Match {
 // One warp-uniform step of the exact parse from state s (s.p + 3 < size):
 // either finds the next match (returns true, s advanced past it, repeat
 // offsets updated) or moves s.p over up to 32 literal positions.
-__device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, const uint16_t *cand, uint32_t size,
-                                          bool lazy, PState &s, Match &m) {
+__device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, CandBuf &cb, uint32_t size, bool lazy,
+                                          PState &s, Match &m) {
     const uint32_t lane = lane_id();
     const uint32_t p = s.p;
     const uint32_t lim = size - 3u - p;
@@ -150,9 +226,7 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, cons
     uint32_t H = __funnelshift_r(bm[p >> 5], bm[(p >> 5) + 1], p & 31u);
     if (nscan < 32u) H &= (1u << nscan) - 1u;
     const uint32_t q = p + lane;
-    // The candidates of the 32 positions, and of p+32 for a lazy step at lane 31.
-    const uint32_t cq = q < size ? static_cast<uint32_t>(cand[q]) : 0u;
-    const uint32_t c32 = p + 32u < size ? static_cast<uint32_t>(cand[p + 32u]) : 0u;
+    cb.advance(p);  // candidates of p .. p+32 (and the next block in flight)
     uint32_t f, rsel = 0;
     bool hash;
     if (H & 1u) {
@@ -182,26 +256,31 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, cons
         }
     }
     const uint32_t fi = f - p;
-    const uint32_t cf = zmap(__shfl_sync(kFull, cq, fi));
-    const uint32_t cs = __shfl_sync(kFull, cq, (fi + 1u) & 31u);
-    const uint32_t cf1 = zmap(fi + 1u < 32u ? cs : c32);
-    uint32_t off, len;
+    const uint32_t cf = zmap(cb.get(f));
+    const uint32_t cf1 = zmap(cb.get(f + 1u));
+    uint32_t off, c0;
     if (hash) {
         off = f - cf;
-        len = extend_warp(w, cf + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
+        c0 = cf;
     } else {  // first repeat offset with 3 equal bytes wins
         const uint32_t r = __shfl_sync(kFull, rsel, fi);
         off = r == 0u ? s.r0 : (r == 1u ? s.r1 : s.r2);
-        len = extend_warp(w, f - off + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
+        c0 = f - off;
     }
-    if (lazy && f + 4u < size && bm_bit(bm, f + 1u)) {
-        const uint32_t len2 =
-            extend_warp(w, cf1 + kMinMatch, f + 1u + kMinMatch, size - f - 1u - kMinMatch) + kMinMatch;
+    uint32_t len;
+    if (lazy && f + 4u < size && bm_bit(bm, f + 1u)) {  // main match and lazy candidate together
+        uint32_t l1, l2;
+        extend_pair(w, c0 + kMinMatch, f + kMinMatch, size - f - kMinMatch, cf1 + kMinMatch, f + 1u + kMinMatch,
+                    size - f - 1u - kMinMatch, l1, l2);
+        len = l1 + kMinMatch;
+        const uint32_t len2 = l2 + kMinMatch;
         if (len2 > len + 1u) {
             f += 1u;
             len = len2;
             off = f - cf1;
         }
+    } else {
+        len = extend_warp(w, c0 + kMinMatch, f + kMinMatch, size - f - kMinMatch) + kMinMatch;
     }
     m.start = f;
     m.len = len;
@@ -242,7 +321,7 @@ struct ListWriter {
 
 // ---------------------------------------------------------------- kernel
 template <bool kRef>
-__global__ void __launch_bounds__(kThreads) zstd_parse_kernel(Zstd2Args a) {
+__global__ void __launch_bounds__(kThreads, 3) zstd_parse_kernel(Zstd2Args a) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     SmemLayout &S = *reinterpret_cast<SmemLayout *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -304,11 +383,13 @@ __global__ void __launch_bounds__(kThreads) zstd_parse_kernel(Zstd2Args a) {
         const bool last_active = !(seg_end < lim_pos);
         ListWriter lw(seg + warp * kLaneCap);
         PState s{seg_start, 1u, 4u, 8u};
+        CandBuf cb{cand, size, 0u, 0u, 0u, 0u};
+        if (active) cb.init(seg_start);
         if (active) {
             const uint32_t stop = last_active ? size : seg_end;
             Match m;
             while (s.p < stop && s.p + 3u < size) {
-                if (warp_step(win, S.bm, cand, size, lazy, s, m)) lw.put(pack_entry(m));
+                if (warp_step(win, S.bm, cb, size, lazy, s, m)) lw.put(pack_entry(m));
             }
             lw.flush();
         }
@@ -326,7 +407,7 @@ __global__ void __launch_bounds__(kThreads) zstd_parse_kernel(Zstd2Args a) {
             uint32_t t = kNoWarp, j = 0;
             Match m;
             while (s.p + 3u < size) {
-                if (!warp_step(win, S.bm, cand, size, lazy, s, m)) continue;
+                if (!warp_step(win, S.bm, cb, size, lazy, s, m)) continue;
                 const uint32_t tw = m.start / kSegW;  // warp whose segment holds this match start
                 if (tw != t) {
                     t = tw;
@@ -463,10 +544,12 @@ __global__ void __launch_bounds__(kThreads) zstd_parse_kernel(Zstd2Args a) {
         } else if (warp == 0) {
             // ---- exact warp-wide parse of the whole window
             PState fs{0u, 1u, 4u, 8u};
+            CandBuf fcb{cand, size, 0u, 0u, 0u, 0u};
+            fcb.init(0u);
             uint32_t idx = 0, cov = 0, prev_end = 0;
             Match m;
             while (fs.p + 3u < size) {
-                if (!warp_step(win, S.bm, cand, size, lazy, fs, m)) continue;
+                if (!warp_step(win, S.bm, fcb, size, lazy, fs, m)) continue;
                 if (idx < a.max_seqs && lane == 0) {
                     const uint32_t ll = m.start - prev_end;
                     if constexpr (kRef) {

@@ -72,7 +72,8 @@ const char *gcz_version(void);
  * the candidate sweep then the per-window second stage, 1 the fused
  * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
  * memory with bulk copies, 0 reads it through L1; "parse_ctas" = second-stage
- * CTAs per SM (1-8). */
+ * CTAs per SM (1-8); "slice_windows" = windows per slice of the host-buffer
+ * pipeline (default 1024 = 64 MiB; two slices are in flight). */
 int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
 /* Read a knob or a counter: "algo" (1: fused single-warp kernels, 2: candidate
  * sweep + second stage, the default), "fallback_windows" (Zstd windows whose
