@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--bytes", type=int, default=N_BYTES, help="input bytes per GPU (profiling runs use less)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--algo", type=int, default=2, help="1: fused single-warp kernels, 2: sweep + second stage")
+    ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2"],
+                    help="zstd: Zstd L2 batched 1 GiB (the reported line); lzma2: LZMA2 L1 1 GiB, seed 3")
     return ap.parse_args()
 
 
@@ -153,6 +155,15 @@ def sum_over_ranks(dist, torch, value):
     return float(t.item())
 
 
+def measured_traffic(workload, n):
+    """DRAM bytes per step from the committed ncu summary (1 GiB step), or None."""
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if n != N_BYTES or not os.path.exists(tfile):
+        return None
+    with open(tfile) as f:
+        return json.load(f).get(workload)
+
+
 def cpu_oracle_time(data, depth, threads):
     from oracle import oracle as orc
 
@@ -236,11 +247,7 @@ def run_gcz(args):
     step_ms = kern_ms / max(kern_launches, 1)
     alg_bytes = n + 16 * nseq + 8 * B  # input once + ZSTD_Sequence out + counts/offsets
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
-    traffic = None
-    tfile = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tfile):
-        with open(tfile) as f:
-            traffic = json.load(f).get(WORKLOAD)
+    traffic = measured_traffic(WORKLOAD, n)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -271,6 +278,81 @@ def run_gcz(args):
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_lzma2(args):
+    """LZMA2 L1 workload: 1 GiB (seed 3, copy offsets to 128 MiB), 16384
+    windows, per-position packed matches + per-window has-match byte."""
+    import torch
+    import gcz
+
+    world, rank, local, dist = dist_setup(args)
+    dev = torch.device("cuda", local)
+    ctx = gcz.Context(local)
+    ctx.set_option("algo", args.algo)
+    n = args.bytes
+    data = gcz.gen_synthetic(3 + 1000 * rank, n, 128 << 20)
+    B = gcz.num_windows(n)
+    d_in = torch.from_numpy(data).to(dev)
+    d_packed = torch.empty(n, dtype=torch.int32, device=dev)
+    d_has = torch.empty(B, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        ctx.lzma2_match_find_device(d_in.data_ptr(), n, 32, d_packed.data_ptr(), d_has.data_ptr(), sp)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.sync(sp)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist, torch, local)
+    with Clocks(local) as clk:
+        ctx.profile_start()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        kern_ms, kern_launches, all_launches = ctx.profile_stop()
+    barrier(dist, torch, local)
+    ms_max = max_over_ranks(dist, torch, e0.elapsed_time(e1))
+    value = world * n * args.steps / (ms_max / 1e3) / 1e9
+    e2e_value = None
+    if args.e2e_steps > 0:
+        h_in = torch.from_numpy(data).pin_memory()
+        h_packed = torch.empty(n, dtype=torch.int32).pin_memory()
+        h_has = torch.empty(B, dtype=torch.uint8).pin_memory()
+
+        def e2e_step():
+            rc = gcz.L.gcz_lzma2_match_find(ctx.handle, h_in.data_ptr(), n, 32, h_packed.data_ptr(), h_has.data_ptr())
+            if rc != 0:
+                raise RuntimeError(gcz.L.gcz_last_error(ctx.handle).decode())
+
+        e2e_step()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e2e_value = round(world * n * args.e2e_steps / max_over_ranks(dist, torch, time.perf_counter() - t0) / 1e9, 3)
+    peak, peak_kind = peaks()
+    step_ms = kern_ms / max(kern_launches, 1)
+    alg_bytes = n + 4 * n + B  # input once + packed matches + has-match bytes
+    achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": "input GB/s per B200 (LZMA2 L1 match-find)", "value": round(value, 3), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generator)",
+            "config": {"workload": "lzma2_l1_1gib", "input_bytes_per_gpu": n, "windows_per_gpu": B, "algo": args.algo},
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": 4 * n + B},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": measured_traffic("lzma2_l1_1gib", n),
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "kernel_ms_per_step": round(step_ms, 4), "algorithmic_bytes_per_step": alg_bytes},
+            "gpu_launches": int(all_launches), "clocks": clk.summary()}), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
@@ -361,6 +443,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "lzma2":
+        run_lzma2(args)
     else:
         run_gcz(args)
 
