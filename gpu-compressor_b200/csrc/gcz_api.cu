@@ -171,22 +171,25 @@ size_t nwin(size_t n) { return (n + kW - 1) / kW; }
 
 // Zstd on device memory for one contiguous range of windows: packed sequences
 // into ctx scratch, counts, offsets (num+1, relative), compact expansion.
+// With `wins`, n is the slab size and nbw the number of windows in the table.
 int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, uint32_t depth, void *d_seqs,
-                     uint64_t capacity, uint64_t *d_offsets, cudaStream_t st) {
-    const size_t nb = nwin(n);
+                     uint64_t capacity, uint64_t *d_offsets, cudaStream_t st, const gcz::WinDesc *wins = nullptr,
+                     size_t nbw = 0) {
+    const size_t nb = wins ? nbw : nwin(n);
     int r;
     if ((r = ensure_dev(c, sc.packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
     if ((r = ensure_dev(c, sc.counts, nb * 4)) != GCZ_OK) return r;
     uint32_t *counts = static_cast<uint32_t *>(sc.counts.p);
-    if (c->algo == 2) {
+    const bool split = c->algo == 2 || wins;  // window tables run on the split kernels only
+    if (split) {
         if ((r = ensure_dev(c, sc.cand, n * 2 + 64)) != GCZ_OK) return r;
         if ((r = ensure_dev(c, sc.seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
     }
     // The profiled interval covers the whole match-find step (all its kernels).
     ProfScope ps(c, st);
-    if (c->algo == 2) {
+    if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
-        GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st, wins));
         gcz::Zstd2Launch l{};
         l.src = d_src;
         l.cand = cand;
@@ -201,6 +204,7 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
         l.status = c->d_status;
         l.num_sms = c->num_sms;
         l.ctas_per_sm = c->parse_ctas;
+        l.wins = wins;
         GCZ_CUDA(c, gcz::launch_zstd_parse(l, st));
         c->all_launches += 2;
     } else {
@@ -228,11 +232,12 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
 
 int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st) {
     int r;
-    if (c->algo == 2 && (r = ensure_dev(c, sc.cand, l.n * 2 + 64)) != GCZ_OK) return r;
+    const bool split = c->algo == 2 || l.wins;
+    if (split && (r = ensure_dev(c, sc.cand, l.n * 2 + 64)) != GCZ_OK) return r;
     ProfScope ps(c, st);
-    if (c->algo == 2) {
+    if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
-        GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st, l.wins));
         GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, st));
         c->all_launches += 2;
     } else {
@@ -682,6 +687,124 @@ extern "C" int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *c, const uint8_t 
     l.num_sms = c->num_sms;
     l.staged = c->staged;
     return lzma_run(c, c->sc, l, st);
+}
+
+// =========================================================================== batches
+
+static_assert(sizeof(gcz_window) == sizeof(gcz::WinDesc), "gcz_window mirrors the kernels' window table");
+
+extern "C" size_t gcz_batch_num_windows(const size_t *sizes, size_t count) {
+    size_t nb = 0;
+    for (size_t i = 0; sizes && i < count; i++) nb += nwin(sizes[i]);
+    return nb;
+}
+
+extern "C" int gcz_batch_layout(const size_t *sizes, size_t count, uint64_t *file_offsets, gcz_window *windows,
+                                uint64_t *slab_bytes) {
+    if ((count && !sizes) || !slab_bytes) return GCZ_EINVAL;
+    uint64_t off = 0;
+    size_t w = 0;
+    for (size_t i = 0; i < count; i++) {
+        off = (off + 15u) & ~uint64_t(15);
+        if (file_offsets) file_offsets[i] = off;
+        for (uint64_t s = 0; s < sizes[i]; s += kW, ++w) {
+            if (windows) {
+                windows[w].offset = off + s;
+                windows[w].size = (uint32_t)std::min<uint64_t>(kW, sizes[i] - s);
+                windows[w].file = (uint32_t)i;
+            }
+        }
+        off += sizes[i];
+    }
+    *slab_bytes = (off + 15u) & ~uint64_t(15);
+    return GCZ_OK;
+}
+
+extern "C" int gcz_zstd_match_find_batch_device(gcz_ctx *c, const uint8_t *d_slab, uint64_t slab_bytes,
+                                                const gcz_window *d_windows, uint32_t num_windows,
+                                                uint32_t search_depth, gcz_zstd_sequence *d_seqs,
+                                                size_t seq_capacity, uint64_t *d_offsets, void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!d_offsets || (num_windows && (!d_slab || !d_windows || !d_seqs))) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_slab)) return fail(c, GCZ_EINVAL, "d_slab must be 16-byte aligned");
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    if (num_windows == 0) {
+        GCZ_CUDA(c, cudaMemsetAsync(d_offsets, 0, 8, st));
+        return GCZ_OK;
+    }
+    return zstd_device_core(c, c->sc, d_slab, slab_bytes, search_depth, d_seqs, seq_capacity, d_offsets, st,
+                            reinterpret_cast<const gcz::WinDesc *>(d_windows), num_windows);
+}
+
+extern "C" int gcz_lzma2_match_find_batch_device(gcz_ctx *c, const uint8_t *d_slab, uint64_t slab_bytes,
+                                                 const gcz_window *d_windows, uint32_t num_windows,
+                                                 uint32_t search_depth, uint32_t *d_packed, uint8_t *d_has_matches,
+                                                 void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (num_windows && (!d_slab || !d_windows)) return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_slab)) return fail(c, GCZ_EINVAL, "d_slab must be 16-byte aligned");
+    DeviceGuard g(c->device);
+    if (num_windows == 0) return GCZ_OK;
+    gcz::LzmaLaunch l{};
+    l.src = d_slab;
+    l.n = slab_bytes;
+    l.window = kW;
+    l.num_windows = num_windows;
+    l.search_depth = search_depth;
+    l.max_matches = GCZ_LZMA2_MAX_MATCHES;
+    l.packed = d_packed;
+    l.has_matches = d_has_matches;
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    l.staged = 1;
+    l.wins = reinterpret_cast<const gcz::WinDesc *>(d_windows);
+    return lzma_run(c, c->sc, l, pick_stream(c, stream));
+}
+
+extern "C" int gcz_zstd_match_find_files(gcz_ctx *c, const uint8_t *const *srcs, const size_t *sizes, size_t count,
+                                         uint32_t search_depth, gcz_zstd_sequence *seqs, size_t seq_capacity,
+                                         uint64_t *window_offsets) {
+    if (!c) return GCZ_EINVAL;
+    if ((count && (!srcs || !sizes)) || !window_offsets) return fail(c, GCZ_EINVAL, "null pointer");
+    const size_t nb = gcz_batch_num_windows(sizes, count);
+    if (nb > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "too many windows");
+    std::vector<uint64_t> foff(count);
+    std::vector<gcz_window> wins(nb);
+    uint64_t slab = 0;
+    gcz_batch_layout(sizes, count, foff.data(), wins.data(), &slab);
+    window_offsets[0] = 0;
+    if (nb == 0) return GCZ_OK;
+    int r;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        Slot &sl = c->slots[0];
+        if ((r = ensure_dev(c, sl.in, slab + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.lz_has, nb * sizeof(gcz_window))) != GCZ_OK) return r;  // window table
+        if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
+        size_t cap = 0;
+        for (size_t i = 0; i < count; i++) cap += gcz_zstd_max_sequences(sizes[i]);
+        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
+        uint8_t *slab_p = static_cast<uint8_t *>(sl.in.p);
+        for (size_t i = 0; i < count; i++)
+            if (sizes[i]) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + foff[i], srcs[i], sizes[i], cudaMemcpyHostToDevice, sl.st));
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.lz_has.p, wins.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, sl.st));
+        if ((r = zstd_device_core(c, sl.sc, slab_p, slab, search_depth, sl.seqs.p, cap,
+                                  static_cast<uint64_t *>(sl.offsets.p), sl.st,
+                                  static_cast<const gcz::WinDesc *>(sl.lz_has.p), nb)) != GCZ_OK)
+            return r;
+        GCZ_CUDA(c, cudaMemcpyAsync(window_offsets, sl.offsets.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+        GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+        const uint64_t total = window_offsets[nb];
+        if (total > seq_capacity)
+            return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)total, seq_capacity);
+        if (total) GCZ_CUDA(c, cudaMemcpyAsync(seqs, sl.seqs.p, total * 16, cudaMemcpyDeviceToHost, sl.st));
+        GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+        return read_status(c, sl.st);
+    }
 }
 
 // =========================================================================== profiling

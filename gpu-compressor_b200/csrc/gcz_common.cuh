@@ -72,6 +72,21 @@ struct GlobalWin {
     }
 };
 
+// Sets a kernel's dynamic shared-memory limit once per device (host side), so
+// that later launches -- including ones being captured into a CUDA graph --
+// make no attribute calls.
+template <class Kernel>
+inline cudaError_t set_smem_once(Kernel k, uint32_t bytes, unsigned long long &done_mask) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done_mask & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e == cudaSuccess) done_mask |= bit;
+    return e;
+}
+
 // ---------------------------------------------------------------------------
 // mbarrier + 1-D bulk copy (TMA, no tensor map, no multicast).
 // ---------------------------------------------------------------------------

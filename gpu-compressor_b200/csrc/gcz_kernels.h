@@ -6,6 +6,15 @@
 
 namespace gcz {
 
+// One window of a batched launch: bytes [offset, offset + size) of the input
+// slab (offset 16-byte aligned, size <= 65536).  Windows of one file follow
+// each other at 64 KiB steps; the last one may be short.
+struct WinDesc {
+    uint64_t offset;
+    uint32_t size;
+    uint32_t file;
+};
+
 struct ZstdLaunch {
     const uint8_t *src;     // 16-byte aligned
     uint64_t n;
@@ -36,6 +45,7 @@ struct LzmaLaunch {
     uint32_t *status;
     int num_sms;
     int staged;
+    const WinDesc *wins = nullptr;  // optional window table (second stage only)
 };
 
 // Second-stage Zstd parse after the candidate sweep.
@@ -55,11 +65,12 @@ struct Zstd2Launch {
     uint32_t *status;       // [0] error bits, [1] windows that took the exact fallback
     int num_sms;
     int ctas_per_sm;
+    const WinDesc *wins;    // optional window table (null: windows at window * w)
 };
 
 cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st);
+                              int num_sms, cudaStream_t st, const WinDesc *wins = nullptr);
 size_t zstd2_seg_scratch_entries(uint32_t num_windows);
 cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st);
 cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);

@@ -222,6 +222,7 @@ struct L2Args {
     uint32_t *ref_matches;
     uint32_t *ref_counts;
     uint32_t *status;
+    const WinDesc *wins;
 };
 
 __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
@@ -238,8 +239,9 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
     __syncthreads();
     SmemWin win{reinterpret_cast<const uint32_t *>(S.data + kL2Pre)};
     for (uint32_t wi = blockIdx.x; wi < a.num_windows; wi += gridDim.x) {
-        const uint64_t start = static_cast<uint64_t>(wi) * a.window;
-        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        const uint64_t start = a.wins ? a.wins[wi].offset : static_cast<uint64_t>(wi) * a.window;
+        const uint32_t size =
+            a.wins ? a.wins[wi].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
         __syncthreads();
         if (tid == 0) {
             S.any = 0;
@@ -345,11 +347,11 @@ cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st) {
     const uint32_t smem = staged ? kSmemStaged : kSmemTable;
     cudaError_t e;
     if (staged) {
-        e = cudaFuncSetAttribute(lzma_match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        { static unsigned long long smem_set_1 = 0; e = set_smem_once(lzma_match_kernel<true>, smem, smem_set_1); }
         if (e != cudaSuccess) return e;
         lzma_match_kernel<true><<<grid, 32, smem, st>>>(a);
     } else {
-        e = cudaFuncSetAttribute(lzma_match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        { static unsigned long long smem_set_2 = 0; e = set_smem_once(lzma_match_kernel<false>, smem, smem_set_2); }
         if (e != cudaSuccess) return e;
         lzma_match_kernel<false><<<grid, 32, smem, st>>>(a);
     }
@@ -379,8 +381,10 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     a.ref_matches = l.ref_matches;
     a.ref_counts = l.ref_counts;
     a.status = l.status;
+    a.wins = l.wins;
     const uint32_t smem = sizeof(L2Smem);
-    cudaError_t e = cudaFuncSetAttribute(lzma_verify_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static unsigned long long smem_set_3 = 0;
+    cudaError_t e = set_smem_once(lzma_verify_kernel, smem, smem_set_3);
     if (e != cudaSuccess) return e;
     int grid = l.num_sms * 3;
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);

@@ -33,6 +33,7 @@ struct SweepArgs {
     uint32_t window;
     uint32_t num_windows;
     uint16_t *cand;  // one entry per input byte, same offsets as src
+    const WinDesc *wins;
 };
 
 __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(SweepArgs a) {
@@ -43,8 +44,9 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
     const uint32_t gwarps = gridDim.x * kSweepWarpsPerCta;
     for (uint32_t w = blockIdx.x * kSweepWarpsPerCta + warp; w < a.num_windows; w += gwarps) {
-        const uint64_t start = static_cast<uint64_t>(w) * a.window;
-        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        const uint64_t start = a.wins ? a.wins[w].offset : static_cast<uint64_t>(w) * a.window;
+        const uint32_t size =
+            a.wins ? a.wins[w].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
         for (uint32_t i = lane; i < kHashSize * 2 / 16; i += 32) T4[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
         __syncwarp();
         const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);
@@ -125,11 +127,12 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
 }  // namespace
 
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st) {
+                              int num_sms, cudaStream_t st, const WinDesc *wins) {
     if (num_windows == 0) return cudaSuccess;
-    SweepArgs a{src, n, window, num_windows, cand};
+    SweepArgs a{src, n, window, num_windows, cand, wins};
     const uint32_t smem = kSweepWarpsPerCta * kHashSize * sizeof(uint16_t);
-    cudaError_t e = cudaFuncSetAttribute(cand_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    static unsigned long long smem_set_1 = 0;
+    cudaError_t e = set_smem_once(cand_sweep_kernel, smem, smem_set_1);
     if (e != cudaSuccess) return e;
     uint32_t ctas = (num_windows + kSweepWarpsPerCta - 1) / kSweepWarpsPerCta;
     if (ctas > static_cast<uint32_t>(num_sms)) ctas = num_sms;

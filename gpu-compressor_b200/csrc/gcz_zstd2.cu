@@ -89,6 +89,7 @@ struct Zstd2Args {
     uint32_t *seq_counts;
     uint32_t *lit_counts;
     uint32_t *status;
+    const WinDesc *wins;
 };
 
 // ---------------------------------------------------------------- helpers
@@ -336,8 +337,9 @@ __global__ void __launch_bounds__(kThreads, 3) zstd_parse_kernel(Zstd2Args a) {
     const bool lazy = a.lazy != 0;
 
     for (uint32_t wi = blockIdx.x; wi < a.num_windows; wi += gridDim.x) {
-        const uint64_t start = static_cast<uint64_t>(wi) * a.window;
-        const uint32_t size = static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        const uint64_t start = a.wins ? a.wins[wi].offset : static_cast<uint64_t>(wi) * a.window;
+        const uint32_t size =
+            a.wins ? a.wins[wi].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
         const uint16_t *cand = a.cand + start;
         uint2 *seg = a.seg + static_cast<uint64_t>(wi) * kWarps * kLaneCap;
 
@@ -597,17 +599,18 @@ cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st) {
     a.seq_counts = l.seq_counts;
     a.lit_counts = l.lit_counts;
     a.status = l.status;
+    a.wins = l.wins;
     const uint32_t smem = sizeof(SmemLayout);
     static_assert(sizeof(SmemLayout) + 1024 <= 233472 / 3, "three CTAs per SM must fit");
     int grid = l.num_sms * l.ctas_per_sm;
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
     cudaError_t e;
     if (l.ref_seqs) {
-        e = cudaFuncSetAttribute(zstd_parse_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        { static unsigned long long smem_set_1 = 0; e = set_smem_once(zstd_parse_kernel<true>, smem, smem_set_1); }
         if (e != cudaSuccess) return e;
         zstd_parse_kernel<true><<<grid, kThreads, smem, st>>>(a);
     } else {
-        e = cudaFuncSetAttribute(zstd_parse_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        { static unsigned long long smem_set_2 = 0; e = set_smem_once(zstd_parse_kernel<false>, smem, smem_set_2); }
         if (e != cudaSuccess) return e;
         zstd_parse_kernel<false><<<grid, kThreads, smem, st>>>(a);
     }

@@ -165,6 +165,32 @@ class Context:
                                                              num_sub_blocks, total_input_size, max_matches_per_pos,
                                                              search_depth, _stream(stream)))
 
+    # ------------------------------------------------------------ batches
+    def zstd_match_find_files(self, files, search_depth=16):
+        """Many host inputs in one launch: ZSTD_Sequence records u32[N, 4] and
+        per-window offsets u64[W+1] (windows of all files, in file order)."""
+        arrs = [_u8(f) for f in files]
+        k = len(arrs)
+        sizes = (ctypes.c_size_t * k)(*[a.size for a in arrs])
+        ptrs = (ctypes.c_void_p * k)(*[a.ctypes.data if a.size else None for a in arrs])
+        nb = int(L.gcz_batch_num_windows(sizes, k))
+        cap = sum(int(L.gcz_zstd_max_sequences(a.size)) for a in arrs)
+        seqs = np.empty((max(cap, 1), 4), np.uint32)
+        offsets = np.zeros(nb + 1, np.uint64)
+        self._check(L.gcz_zstd_match_find_files(self._h, ptrs, sizes, k, search_depth, seqs.ctypes.data, cap,
+                                                offsets.ctypes.data))
+        return seqs[:int(offsets[-1])], offsets
+
+    def zstd_match_find_batch_device(self, d_slab, slab_bytes, d_windows, num_windows, search_depth, d_seqs,
+                                     capacity, d_offsets, stream=None):
+        self._check(L.gcz_zstd_match_find_batch_device(self._h, d_slab, slab_bytes, d_windows, num_windows,
+                                                       search_depth, d_seqs, capacity, d_offsets, _stream(stream)))
+
+    def lzma2_match_find_batch_device(self, d_slab, slab_bytes, d_windows, num_windows, search_depth, d_packed,
+                                      d_has, stream=None):
+        self._check(L.gcz_lzma2_match_find_batch_device(self._h, d_slab, slab_bytes, d_windows, num_windows,
+                                                        search_depth, d_packed, d_has, _stream(stream)))
+
     # ------------------------------------------------------------ timing
     def profile_start(self):
         self._check(L.gcz_profile_start(self._h))
@@ -253,6 +279,24 @@ def gen_synthetic(seed, n, max_offset=8 << 20, mix=(0.4, 0.4, 0.2), out=None):
     if n:
         L.gcz_gen_synthetic(seed, out.ctypes.data, n, max_offset, float(mix[0]), float(mix[1]), float(mix[2]))
     return out
+
+
+WINDOW_DTYPE = np.dtype([("offset", "<u8"), ("size", "<u4"), ("file", "<u4")])  # gcz_window
+
+
+def batch_layout(sizes):
+    """(file offsets u64[k], window table (WINDOW_DTYPE)[W], slab bytes) of a batch."""
+    sizes = [int(x) for x in sizes]
+    k = len(sizes)
+    cs = (ctypes.c_size_t * k)(*sizes)
+    nb = int(L.gcz_batch_num_windows(cs, k))
+    foff = np.zeros(max(k, 1), np.uint64)
+    wins = np.zeros(max(nb, 1), WINDOW_DTYPE)
+    slab = ctypes.c_uint64()
+    rc = L.gcz_batch_layout(cs, k, foff.ctypes.data, wins.ctypes.data, ctypes.byref(slab))
+    if rc != 0:
+        raise GczError(rc, "gcz_batch_layout failed")
+    return foff[:k], wins[:nb], slab.value
 
 
 def gen_file_sizes(seed, count, min_size=4096, max_size=64 << 20):

@@ -46,6 +46,11 @@ SIGNATURES = {
     "gcz_lzma2_match_find_device": (_i, [_vp, _vp, _sz, _u32, _vp, _vp, _vp]),
     "gcz_lzma2_find_matches": (_i, [_vp, _vp, _sz, _u32, _vp, _vp, _vp]),
     "gcz_lzma2_match_find_ref_layout_device": (_i, [_vp, _vp, _vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp]),
+    "gcz_batch_num_windows": (_sz, [_vp, _sz]),
+    "gcz_batch_layout": (_i, [_vp, _sz, _vp, _vp, ctypes.POINTER(_u64)]),
+    "gcz_zstd_match_find_batch_device": (_i, [_vp, _vp, _u64, _vp, _u32, _u32, _vp, _sz, _vp, _vp]),
+    "gcz_lzma2_match_find_batch_device": (_i, [_vp, _vp, _u64, _vp, _u32, _u32, _vp, _vp, _vp]),
+    "gcz_zstd_match_find_files": (_i, [_vp, _vp, _vp, _sz, _u32, _vp, _sz, _vp]),
     "gcz_profile_start": (_i, [_vp]),
     "gcz_profile_stop": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "gcz_gen_synthetic": (None, [_u64, _vp, _u64, _u64, _d, _d, _d]),

@@ -181,6 +181,44 @@ int gcz_lzma2_match_find_ref_layout_device(gcz_ctx *ctx, const uint8_t *d_input,
                                            uint32_t max_matches_per_pos, uint32_t search_depth,
                                            void *stream);
 
+/* ---------------------------------------------------------------- batches */
+
+/* Many inputs of uneven size in one launch.  Each input is cut into 64 KiB
+ * windows exactly as the reference cuts a file (its 8 MiB / 128 MiB pipeline
+ * chunks are multiples of 64 KiB, pipeline.rs:110, pipeline_lzma2.rs:40), so a
+ * batched window gives the same sequences or matches as the same window
+ * processed alone.  Inputs sit in one device slab at 16-byte aligned offsets;
+ * the window table says where each window is. */
+typedef struct {
+    uint64_t offset;  /* first byte of the window in the slab (16-byte aligned) */
+    uint32_t size;    /* 1 .. 65536 */
+    uint32_t file;    /* index of the input the window belongs to */
+} gcz_window;
+
+size_t gcz_batch_num_windows(const size_t *sizes, size_t count);
+/* Slab layout of `count` inputs: file_offsets[count] (may be NULL),
+ * windows[gcz_batch_num_windows] (may be NULL), total slab bytes. */
+int gcz_batch_layout(const size_t *sizes, size_t count, uint64_t *file_offsets, gcz_window *windows,
+                     uint64_t *slab_bytes);
+
+/* Zstd over a window table (device memory): sequences of window w at
+ * d_seqs[d_offsets[w] .. d_offsets[w+1]).  After a first call of the same
+ * sizes it allocates nothing, so it can be enqueued repeatedly or captured. */
+int gcz_zstd_match_find_batch_device(gcz_ctx *ctx, const uint8_t *d_slab, uint64_t slab_bytes,
+                                     const gcz_window *d_windows, uint32_t num_windows, uint32_t search_depth,
+                                     gcz_zstd_sequence *d_seqs, size_t seq_capacity, uint64_t *d_offsets,
+                                     void *stream);
+/* LZMA2 over a window table: packed results at the slab offsets of each
+ * window's bytes (d_packed has slab_bytes entries), one has-match byte per window. */
+int gcz_lzma2_match_find_batch_device(gcz_ctx *ctx, const uint8_t *d_slab, uint64_t slab_bytes,
+                                      const gcz_window *d_windows, uint32_t num_windows, uint32_t search_depth,
+                                      uint32_t *d_packed, uint8_t *d_has_matches, void *stream);
+/* Host inputs: srcs[i] of sizes[i] bytes.  window_offsets has
+ * gcz_batch_num_windows+1 entries (windows in input order). */
+int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const size_t *sizes, size_t count,
+                              uint32_t search_depth, gcz_zstd_sequence *seqs, size_t seq_capacity,
+                              uint64_t *window_offsets);
+
 /* ---------------------------------------------------------------- timing */
 
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this

@@ -1,0 +1,110 @@
+"""Uneven inputs in one launch: every window of a batch gives exactly what the
+same input gives alone (and what the oracle gives), for Zstd and LZMA2; the
+batch call replays inside a CUDA graph; the autotuner keeps results fixed."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def _files(seed, count, max_size):
+    import gcz
+
+    sizes, mix = gcz.gen_file_sizes(seed, count, 1, max_size)
+    return [gcz.gen_synthetic(seed * 1000 + i, int(s), 8 << 20, tuple(mix[i])) for i, s in enumerate(sizes)]
+
+
+def test_zstd_files_equal_alone_and_oracle(ctx):
+    files = _files(5, 120, 700000)
+    files += [np.zeros(0, np.uint8), np.zeros(5, np.uint8), np.full(65536 * 2 + 3, 7, np.uint8)]
+    seqs, offs = ctx.zstd_match_find_files(files, 16)
+    w = 0
+    for f in files:
+        alone_s, alone_o = ctx.zstd_match_find(f, 16)
+        o_s, o_o = orc.zstd_sequences(f, 16)
+        nbf = alone_o.size - 1
+        base = int(offs[w])
+        np.testing.assert_array_equal(offs[w:w + nbf + 1] - base, alone_o)
+        np.testing.assert_array_equal(seqs[base:int(offs[w + nbf])], alone_s)
+        np.testing.assert_array_equal(alone_s, o_s)
+        w += nbf
+    assert w == offs.size - 1
+
+
+def test_lzma2_batch_device_equals_alone(ctx):
+    import torch
+    import gcz
+
+    files = _files(6, 60, 500000)
+    foff, wins, slab = gcz.batch_layout([f.size for f in files])
+    h_slab = np.zeros(slab, np.uint8)
+    for o, f in zip(foff, files):
+        h_slab[int(o):int(o) + f.size] = f
+    d_slab = torch.from_numpy(h_slab).cuda()
+    d_wins = torch.from_numpy(wins.view(np.uint8)).cuda()
+    d_packed = torch.zeros(slab, dtype=torch.int32, device="cuda")
+    d_has = torch.zeros(max(wins.size, 1), dtype=torch.uint8, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    ctx.lzma2_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 32, d_packed.data_ptr(),
+                                      d_has.data_ptr(), st)
+    ctx.sync(st)
+    packed = d_packed.cpu().numpy().view(np.uint32)
+    has = d_has.cpu().numpy()
+    w = 0
+    for o, f in zip(foff, files):
+        alone_p, alone_h = ctx.lzma2_match_find(f, 32)
+        np.testing.assert_array_equal(packed[int(o):int(o) + f.size], alone_p)
+        np.testing.assert_array_equal(packed[int(o):int(o) + f.size], orc.lzma_packed(f, 32))
+        np.testing.assert_array_equal(has[w:w + alone_h.size], alone_h)
+        w += alone_h.size
+
+
+def test_zstd_batch_replays_in_cuda_graph(ctx):
+    import torch
+    import gcz
+
+    files = _files(7, 40, 400000)
+    foff, wins, slab = gcz.batch_layout([f.size for f in files])
+    h_slab = np.zeros(slab, np.uint8)
+    for o, f in zip(foff, files):
+        h_slab[int(o):int(o) + f.size] = f
+    d_slab = torch.from_numpy(h_slab).cuda()
+    d_wins = torch.from_numpy(wins.view(np.uint8)).cuda()
+    cap = sum(int(gcz.L.gcz_zstd_max_sequences(f.size)) for f in files)
+    d_seqs = torch.zeros((cap, 4), dtype=torch.int32, device="cuda")
+    d_off = torch.zeros(wins.size + 1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16, d_seqs.data_ptr(),
+                                         cap, d_off.data_ptr(), s.cuda_stream)  # allocates scratch once
+    torch.cuda.synchronize()
+    want_off = d_off.clone()
+    want = d_seqs[:int(want_off[-1])].clone()
+    d_seqs.zero_()
+    d_off.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16, d_seqs.data_ptr(),
+                                         cap, d_off.data_ptr(), s.cuda_stream)
+    for _ in range(2):
+        d_seqs.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(d_off, want_off)
+        assert torch.equal(d_seqs[:int(want_off[-1])], want)
+    del g
+
+
+def test_autotuner_keeps_results_and_picks_a_config(ctx, tmp_path):
+    import gcz
+    from gcz import autotune
+
+    sample = gcz.gen_synthetic(8, 8 << 20, 8 << 20)
+    out = autotune.tune(ctx, sample, reps=2, save_path=str(tmp_path / "tune.json"))
+    assert out["best"] in [r["config"] for r in out["results"]]
+    assert len(out["results"]) >= 3
+    ctx.set_option("algo", 2)
+    ctx.set_option("parse_ctas", 3)
+    ctx.set_option("staged", 1)
