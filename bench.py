@@ -51,8 +51,14 @@ def parse():
     ap.add_argument("--bytes", type=int, default=N_BYTES, help="input bytes per GPU (profiling runs use less)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--algo", type=int, default=2, help="1: fused single-warp kernels, 2: sweep + second stage")
-    ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2"],
-                    help="zstd: Zstd L2 batched 1 GiB (the reported line); lzma2: LZMA2 L1 1 GiB, seed 3")
+    ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2", "serving", "uneven"],
+                    help="zstd: Zstd L2 batched 1 GiB (the reported line); lzma2: LZMA2 L1 1 GiB, seed 3; "
+                         "serving: open-loop request stream; uneven: many files in one launch")
+    ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second (Poisson)")
+    ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
+    ap.add_argument("--max-request", type=int, default=64 << 20, help="serving: largest request size")
+    ap.add_argument("--files", type=int, default=4096, help="uneven: number of files")
+    ap.add_argument("--max-file", type=int, default=8 << 20, help="uneven: largest file size")
     return ap.parse_args()
 
 
@@ -357,6 +363,159 @@ def run_lzma2(args):
         dist.destroy_process_group()
 
 
+def run_serving(args):
+    """Open-loop Poisson stream against the library's request loop: request
+    sizes log-uniform 4 KiB..max_request, 70% Zstd L1 / 20% Zstd L2 / 10% LZMA2
+    L1, payloads are slices of a pinned 1 GiB synthetic pool.  Reports the
+    completed input GB/s and submit-to-completion p50/p99 latency."""
+    import threading
+    import torch
+    import gcz
+    from gcz import serving
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = gcz.Context(local)
+    pool_n = 1 << 30
+    pool = torch.empty(pool_n, dtype=torch.uint8).pin_memory()
+    gcz.gen_synthetic(5, pool_n, 8 << 20, out=pool.numpy())
+    srv = serving.Server(ctx, hbm_budget=120 * 10**9, max_batch_bytes=1 << 30)
+    rng = np.random.default_rng(11)
+    count = int(args.rate * args.duration)
+    gaps = rng.exponential(1.0 / args.rate, size=count)
+    sizes = np.exp(rng.uniform(np.log(4096), np.log(args.max_request), size=count)).astype(np.int64)
+    u = rng.random(count)
+    kinds = np.where(u < 0.9, serving.ZSTD, serving.LZMA2)
+    depths = np.where(u < 0.7, 16, np.where(u < 0.9, 64, 32))
+    offs = (rng.random(count) * (pool_n - sizes)).astype(np.int64)
+    pool_np = pool.numpy()
+    q = []
+    lock = threading.Condition()
+    # Output buffers: pinned, reused, one free list per power-of-two size class.
+    # Zstd results get room for n/16 + 1024 sequences (this input averages one
+    # sequence per ~50 bytes; a smaller real count never overflows it).
+    free = {}
+    free_lock = threading.Lock()
+
+    def take(cls_bytes):
+        with free_lock:
+            lst = free.setdefault(cls_bytes, [])
+            if lst:
+                return lst.pop()
+        return torch.empty(cls_bytes, dtype=torch.uint8).pin_memory().numpy()
+
+    def give(cls_bytes, buf):
+        with free_lock:
+            free[cls_bytes].append(buf)
+
+    def cls(nbytes):
+        return 1 << max(12, int(nbytes - 1).bit_length())
+
+    def waiter():
+        i = 0
+        while i < count:
+            with lock:
+                while len(q) <= i:
+                    lock.wait()
+                r, bufs = q[i]
+            srv.wait(r)
+            for c, b in bufs:
+                give(c, b)
+            q[i] = None
+            i += 1
+
+    wt = threading.Thread(target=waiter)
+    wt.start()
+    t0 = time.perf_counter()
+    nxt = t0
+    for i in range(count):
+        nxt += gaps[i]
+        d = nxt - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        n = int(sizes[i])
+        nb = gcz.num_windows(n)
+        if kinds[i] == serving.ZSTD:
+            cap = n // 16 + 1024
+            ca, cb = cls(cap * 16), cls((nb + 1) * 8)
+            ba, bb = take(ca), take(cb)
+            r = srv.submit(serving.ZSTD, pool_np[offs[i]:offs[i] + n], int(depths[i]),
+                           out_a=ba.view(np.uint32)[:cap * 4].reshape(cap, 4), cap=cap, out_b=bb.view(np.uint64))
+            bufs = [(ca, ba), (cb, bb)]
+        else:
+            cb = cls(nb)
+            bb = take(cb)
+            r = srv.submit(serving.LZMA2, pool_np[offs[i]:offs[i] + n], 32, out_b=bb, packed=False)
+            bufs = [(cb, bb)]
+        with lock:
+            q.append((r, bufs))
+            lock.notify()
+    wt.join()
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    print(json.dumps({
+        "metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "value": round(st["bytes"] / wall / 1e9, 3),
+        "unit": "GB/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic (seeded pool)",
+        "config": {"workload": "serving_poisson", "rate_per_s": args.rate, "duration_s": args.duration,
+                   "requests": count, "size_range": [4096, args.max_request], "mix": "70% zstd L1, 20% zstd L2, 10% lzma2 (has-match bytes only)",
+                   "outputs": "pinned, reused per size class", "offered_gbps": round(float(sizes.sum()) / args.duration / 1e9, 3), "hbm_budget_bytes": 120 * 10**9,
+                   "max_batch_bytes": 1 << 30},
+        "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3)},
+        "batches": st["batches"], "completed": st["completed"], "wall_s": round(wall, 3)}), flush=True)
+
+
+def run_uneven(args):
+    """Uneven batch: many files of log-uniform size with per-file Dirichlet(1,1,1)
+    mixes in one launch through the window-table entry point (device resident).
+    Reports input GB/s of the launch."""
+    import torch
+    import gcz
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = gcz.Context(local)
+    sizes, mix = gcz.gen_file_sizes(4, args.files, 4096, args.max_file)
+    foff, wins, slab = gcz.batch_layout(sizes)
+    h_slab = torch.zeros(slab, dtype=torch.uint8).pin_memory()
+    hs = h_slab.numpy()
+    from concurrent.futures import ThreadPoolExecutor
+
+    def gen(i):
+        o, sz = int(foff[i]), int(sizes[i])
+        gcz.gen_synthetic(4000 + i, sz, 8 << 20, tuple(mix[i]), out=hs[o:o + sz])
+
+    with ThreadPoolExecutor(os.cpu_count() or 4) as ex:
+        list(ex.map(gen, range(len(sizes))))
+    d_slab = h_slab.cuda()
+    d_wins = torch.from_numpy(wins.view(np.uint8)).cuda()
+    cap = sum(int(gcz.L.gcz_zstd_max_sequences(int(x))) for x in sizes)
+    d_seqs = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+    d_off = torch.empty(wins.size + 1, dtype=torch.int64, device="cuda")
+    st = torch.cuda.current_stream()
+
+    def step():
+        ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16,
+                                         d_seqs.data_ptr(), cap, d_off.data_ptr(), st.cuda_stream)
+
+    for _ in range(3):
+        step()
+    ctx.sync(st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        step()
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    total = int(np.sum(sizes))
+    print(json.dumps({
+        "metric": "uneven-batch input GB/s per B200 (Zstd L1 match-find, one launch)",
+        "value": round(total / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ms, 3),
+        "config": {"workload": "uneven_batch", "files": args.files, "size_range": [4096, args.max_file],
+                   "input_bytes": total, "windows": int(wins.size), "mix": "Dirichlet(1,1,1) per file"}}), flush=True)
+
+
 def run_reference(args):
     """Reference arm: the reference's path on this box.  `value` = its CPU
     restatement (oracle port) on all host threads over a bounded sample of the
@@ -445,6 +604,10 @@ def main():
         run_reference(args)
     elif args.workload == "lzma2":
         run_lzma2(args)
+    elif args.workload == "serving":
+        run_serving(args)
+    elif args.workload == "uneven":
+        run_uneven(args)
     else:
         run_gcz(args)
 

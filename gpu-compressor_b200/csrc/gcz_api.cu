@@ -1,11 +1,15 @@
 // libgcz C ABI (include/gcz.h): context, buffers, host and device entry points.
 #include <algorithm>
+#include <chrono>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "gcz.h"
@@ -805,6 +809,345 @@ extern "C" int gcz_zstd_match_find_files(gcz_ctx *c, const uint8_t *const *srcs,
         GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
         return read_status(c, sl.st);
     }
+}
+
+// =========================================================================== serving
+
+namespace {
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Worst-case device bytes per input byte of one batch: slab 1, candidates 2,
+// Zstd packed 2.67, speculative lists 3.25, ZSTD_Sequence output 5.33.
+constexpr double kDeviceBytesPerInputByte = 14.5;
+
+struct ServerReq {
+    uint64_t id = 0;
+    int kind = 0;
+    uint32_t depth = 0;
+    const uint8_t *src = nullptr;
+    size_t n = 0;
+    void *out_a = nullptr;
+    size_t cap_a = 0;
+    void *out_b = nullptr;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    int status = 1;  // 1 = pending
+    uint32_t w0 = 0, nw = 0;
+    uint64_t slab_off = 0;
+};
+
+struct Batch {
+    std::vector<ServerReq *> reqs;
+    int kind = 0;
+    uint32_t depth = 0;
+    uint32_t nb = 0;
+    bool busy = false;
+};
+
+}  // namespace
+
+struct gcz_server {
+    gcz_ctx *c = nullptr;
+    uint64_t max_batch_bytes = 0;
+    uint32_t max_batch_requests = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<ServerReq *> pending;
+    std::unordered_map<uint64_t, ServerReq *> reqs;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    Slot slots[2];
+    DevBuf wins[2];
+    std::vector<gcz_window> hwins[2];
+    Batch batch[2];
+    std::vector<double> lat_ms;
+    uint64_t completed = 0, bytes_done = 0, batches = 0;
+    int worker_error = GCZ_OK;
+};
+
+namespace {
+
+// Enqueue one batch on its slot: H2D of every request, the window table, the
+// match-find kernels and the copies whose sizes are already known.
+int server_launch(gcz_server *sv, int k) {
+    gcz_ctx *c = sv->c;
+    Batch &b = sv->batch[k];
+    Slot &sl = sv->slots[k];
+    std::vector<gcz_window> &hw = sv->hwins[k];
+    std::vector<size_t> sizes;
+    for (ServerReq *r : b.reqs) sizes.push_back(r->n);
+    std::vector<uint64_t> foff(sizes.size());
+    const size_t nb = gcz_batch_num_windows(sizes.data(), sizes.size());
+    hw.resize(nb);
+    uint64_t slab = 0;
+    gcz_batch_layout(sizes.data(), sizes.size(), foff.data(), hw.data(), &slab);
+    uint32_t w = 0;
+    for (size_t i = 0; i < b.reqs.size(); i++) {
+        b.reqs[i]->slab_off = foff[i];
+        b.reqs[i]->w0 = w;
+        b.reqs[i]->nw = (uint32_t)nwin(sizes[i]);
+        w += b.reqs[i]->nw;
+    }
+    b.nb = (uint32_t)nb;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    int r;
+    if ((r = ensure_dev(c, sl.in, slab + 64)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sv->wins[k], std::max<size_t>(nb, 1) * sizeof(gcz_window))) != GCZ_OK) return r;
+    uint8_t *slab_p = static_cast<uint8_t *>(sl.in.p);
+    for (ServerReq *q : b.reqs)
+        if (q->n) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + q->slab_off, q->src, q->n, cudaMemcpyHostToDevice, sl.st));
+    GCZ_CUDA(c, cudaMemcpyAsync(sv->wins[k].p, hw.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, sl.st));
+    const gcz::WinDesc *dw = static_cast<const gcz::WinDesc *>(sv->wins[k].p);
+    if (b.kind == 0) {
+        size_t cap = 0;
+        for (ServerReq *q : b.reqs) cap += gcz_zstd_max_sequences(q->n);
+        if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
+        if ((r = ensure_host(c, sl.h_off, (nb + 1) * 8)) != GCZ_OK) return r;
+        if ((r = zstd_device_core(c, sl.sc, slab_p, slab, b.depth, sl.seqs.p, cap, static_cast<uint64_t *>(sl.offsets.p),
+                                  sl.st, dw, nb)) != GCZ_OK)
+            return r;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+    } else {
+        if ((r = ensure_dev(c, sl.lz_packed, slab * 4 + 64)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.lz_has, nb + 16)) != GCZ_OK) return r;
+        gcz::LzmaLaunch l{};
+        l.src = slab_p;
+        l.n = slab;
+        l.window = kW;
+        l.num_windows = (uint32_t)nb;
+        l.search_depth = b.depth;
+        l.max_matches = GCZ_LZMA2_MAX_MATCHES;
+        l.packed = static_cast<uint32_t *>(sl.lz_packed.p);
+        l.has_matches = static_cast<uint8_t *>(sl.lz_has.p);
+        l.status = c->d_status;
+        l.num_sms = c->num_sms;
+        l.staged = 1;
+        l.wins = dw;
+        if ((r = lzma_run(c, sl.sc, l, sl.st)) != GCZ_OK) return r;
+        for (ServerReq *q : b.reqs) {
+            if (!q->n) continue;
+            if (q->out_a)
+                GCZ_CUDA(c, cudaMemcpyAsync(q->out_a, static_cast<uint32_t *>(sl.lz_packed.p) + q->slab_off, q->n * 4,
+                                            cudaMemcpyDeviceToHost, sl.st));
+            if (q->out_b)
+                GCZ_CUDA(c, cudaMemcpyAsync(q->out_b, static_cast<uint8_t *>(sl.lz_has.p) + q->w0, q->nw,
+                                            cudaMemcpyDeviceToHost, sl.st));
+        }
+    }
+    GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
+    return GCZ_OK;
+}
+
+// Second half of a batch: wait for it, copy out the Zstd sequences of every
+// request (their counts are known now), complete the requests.
+void server_finish(gcz_server *sv, int k) {
+    gcz_ctx *c = sv->c;
+    Batch &b = sv->batch[k];
+    Slot &sl = sv->slots[k];
+    int r = GCZ_OK;
+    {
+        DeviceGuard g(c->device);
+        if (cudaEventSynchronize(sl.ev) != cudaSuccess) r = GCZ_ECUDA;
+        if (r == GCZ_OK && b.kind == 0) {
+            const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);
+            for (ServerReq *q : b.reqs) {
+                const uint64_t a = ho[q->w0], e = ho[q->w0 + q->nw];
+                uint64_t *ob = static_cast<uint64_t *>(q->out_b);
+                if (ob)
+                    for (uint32_t i = 0; i <= q->nw; i++) ob[i] = ho[q->w0 + i] - a;
+                if (e - a > q->cap_a) {
+                    q->status = GCZ_ECAPACITY;
+                    continue;
+                }
+                if (e > a &&
+                    cudaMemcpyAsync(q->out_a, static_cast<gcz_zstd_sequence *>(sl.seqs.p) + a, (e - a) * 16,
+                                    cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
+                    r = GCZ_ECUDA;
+            }
+            if (cudaStreamSynchronize(sl.st) != cudaSuccess) r = GCZ_ECUDA;
+        }
+        uint32_t h = 0;
+        if (cudaMemcpy(&h, c->d_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) r = GCZ_ECUDA;
+        if (r == GCZ_OK && h) r = GCZ_EDEVICE;
+    }
+    const double t = now_ms();
+    std::lock_guard<std::mutex> lk(sv->mu);
+    for (ServerReq *q : b.reqs) {
+        if (q->status == 1) q->status = r;
+        q->t_done = t;
+        sv->lat_ms.push_back(q->t_done - q->t_submit);
+        sv->completed++;
+        sv->bytes_done += q->n;
+    }
+    sv->batches++;
+    b.reqs.clear();
+    b.busy = false;
+    sv->cv_done.notify_all();
+}
+
+void server_loop(gcz_server *sv) {
+    int k = 0;
+    for (;;) {
+        Batch &b = sv->batch[k];
+        Batch &other = sv->batch[k ^ 1];
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            if (sv->pending.empty() && !sv->stop && !other.busy)
+                sv->cv_work.wait(lk, [&] { return sv->stop || !sv->pending.empty(); });
+            if (sv->pending.empty() && sv->stop && !other.busy) break;
+            // Admit pending requests of the first request's kind (and Zstd lazy
+            // mode) while the batch stays within the byte and count limits.
+            uint64_t bytes = 0;
+            for (auto it = sv->pending.begin(); it != sv->pending.end();) {
+                ServerReq *q = *it;
+                const bool same = b.reqs.empty() ||
+                                  (q->kind == b.kind && (q->kind != 0 || (q->depth > 1) == (b.depth > 1)));
+                if (same && (b.reqs.empty() || (bytes + q->n <= sv->max_batch_bytes &&
+                                                b.reqs.size() < sv->max_batch_requests))) {
+                    if (b.reqs.empty()) {
+                        b.kind = q->kind;
+                        b.depth = q->depth;
+                    }
+                    q->t_admit = now_ms();
+                    bytes += q->n;
+                    b.reqs.push_back(q);
+                    it = sv->pending.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        if (!b.reqs.empty()) {
+            const int r = server_launch(sv, k);
+            b.busy = true;
+            if (r != GCZ_OK) {
+                std::lock_guard<std::mutex> lk(sv->mu);
+                for (ServerReq *q : b.reqs) q->status = r;
+                sv->worker_error = r;
+            }
+        }
+        if (other.busy) server_finish(sv, k ^ 1);  // overlaps with batch k on the GPU
+        if (!b.reqs.empty()) k ^= 1;
+    }
+    for (int j = 0; j < 2; j++)
+        if (sv->batch[j].busy) server_finish(sv, j);
+}
+
+}  // namespace
+
+extern "C" int gcz_server_create(gcz_ctx *c, uint64_t hbm_budget, uint64_t max_batch_bytes,
+                                 uint32_t max_batch_requests, gcz_server **out) {
+    if (!c || !out) return GCZ_EINVAL;
+    *out = nullptr;
+    gcz_server *sv = new gcz_server();
+    sv->c = c;
+    uint64_t cap = (uint64_t)(hbm_budget / (2.0 * kDeviceBytesPerInputByte));
+    if (max_batch_bytes == 0 || max_batch_bytes > cap) max_batch_bytes = cap;
+    sv->max_batch_bytes = max_batch_bytes & ~uint64_t(kW - 1);
+    if (sv->max_batch_bytes < kW) {
+        delete sv;
+        return fail(c, GCZ_EINVAL, "HBM budget too small for one 64 KiB window per batch");
+    }
+    sv->max_batch_requests = max_batch_requests ? max_batch_requests : 65536;
+    {
+        DeviceGuard g(c->device);
+        for (Slot &sl : sv->slots)
+            if (cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                delete sv;
+                return GCZ_ECUDA;
+            }
+    }
+    sv->worker = std::thread(server_loop, sv);
+    *out = sv;
+    return GCZ_OK;
+}
+
+extern "C" void gcz_server_destroy(gcz_server *sv) {
+    if (!sv) return;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+    }
+    sv->cv_work.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    {
+        DeviceGuard g(sv->c->device);
+        for (int j = 0; j < 2; j++) {
+            Slot &sl = sv->slots[j];
+            for (DevBuf *b : {&sl.sc.packed, &sl.sc.counts, &sl.sc.cand, &sl.sc.seg, &sl.in, &sl.offsets, &sl.seqs,
+                              &sl.lz_packed, &sl.lz_has, &sv->wins[j]})
+                if (b->p) cudaFree(b->p);
+            if (sl.h_off.p) cudaFreeHost(sl.h_off.p);
+            if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.st) cudaStreamDestroy(sl.st);
+        }
+    }
+    for (auto &kv : sv->reqs) delete kv.second;
+    delete sv;
+}
+
+extern "C" uint64_t gcz_server_max_batch_bytes(const gcz_server *sv) { return sv ? sv->max_batch_bytes : 0; }
+
+extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth, const uint8_t *src, size_t n,
+                                 void *out_a, size_t cap_a, void *out_b, uint64_t *id) {
+    if (!sv || !id || (kind != GCZ_REQ_ZSTD && kind != GCZ_REQ_LZMA2) || (n && !src)) return GCZ_EINVAL;
+    if (kind == GCZ_REQ_ZSTD && (!out_b || (n && !out_a))) return GCZ_EINVAL;
+    if (n > sv->max_batch_bytes) return GCZ_ETOOLARGE;
+    ServerReq *q = new ServerReq();
+    q->kind = kind;
+    q->depth = search_depth;
+    q->src = src;
+    q->n = n;
+    q->out_a = out_a;
+    q->cap_a = cap_a;
+    q->out_b = out_b;
+    q->t_submit = now_ms();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        q->id = sv->next_id++;
+        sv->reqs[q->id] = q;
+        sv->pending.push_back(q);
+        *id = q->id;
+    }
+    sv->cv_work.notify_one();
+    return GCZ_OK;
+}
+
+extern "C" int gcz_server_wait(gcz_server *sv, uint64_t id, double timeout_s, double *latency_ms) {
+    if (!sv) return GCZ_EINVAL;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(id);
+    if (it == sv->reqs.end()) return GCZ_EINVAL;
+    ServerReq *q = it->second;
+    const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return q->status != 1; });
+    if (!ok) return GCZ_EDEVICE;
+    const int st = q->status;
+    if (latency_ms) *latency_ms = q->t_done - q->t_submit;
+    sv->reqs.erase(it);
+    delete q;
+    return st;
+}
+
+extern "C" int gcz_server_stats(gcz_server *sv, uint64_t *completed, uint64_t *bytes, uint64_t *batches,
+                                double *p50_ms, double *p99_ms) {
+    if (!sv) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    std::vector<double> v = sv->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double p) { return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))]; };
+    if (completed) *completed = sv->completed;
+    if (bytes) *bytes = sv->bytes_done;
+    if (batches) *batches = sv->batches;
+    if (p50_ms) *p50_ms = pct(0.50);
+    if (p99_ms) *p99_ms = pct(0.99);
+    return sv->worker_error;
 }
 
 // =========================================================================== profiling

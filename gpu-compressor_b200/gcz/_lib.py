@@ -51,6 +51,13 @@ SIGNATURES = {
     "gcz_zstd_match_find_batch_device": (_i, [_vp, _vp, _u64, _vp, _u32, _u32, _vp, _sz, _vp, _vp]),
     "gcz_lzma2_match_find_batch_device": (_i, [_vp, _vp, _u64, _vp, _u32, _u32, _vp, _vp, _vp]),
     "gcz_zstd_match_find_files": (_i, [_vp, _vp, _vp, _sz, _u32, _vp, _sz, _vp]),
+    "gcz_server_create": (_i, [_vp, _u64, _u64, _u32, ctypes.POINTER(_vp)]),
+    "gcz_server_destroy": (None, [_vp]),
+    "gcz_server_max_batch_bytes": (_u64, [_vp]),
+    "gcz_server_submit": (_i, [_vp, _i, _u32, _vp, _sz, _vp, _sz, _vp, ctypes.POINTER(_u64)]),
+    "gcz_server_wait": (_i, [_vp, _u64, _d, ctypes.POINTER(_d)]),
+    "gcz_server_stats": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64),
+                              ctypes.POINTER(_d), ctypes.POINTER(_d)]),
     "gcz_profile_start": (_i, [_vp]),
     "gcz_profile_stop": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "gcz_gen_synthetic": (None, [_u64, _vp, _u64, _u64, _d, _d, _d]),

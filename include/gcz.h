@@ -219,6 +219,35 @@ int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const si
                               uint32_t search_depth, gcz_zstd_sequence *seqs, size_t seq_capacity,
                               uint64_t *window_offsets);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A request loop over one context: requests of mixed kind and size are
+ * submitted at any time and admitted into the next batch while its input stays
+ * within max_batch_bytes (derived from hbm_budget: two batches are in flight,
+ * each needing at most ~14.5 device bytes per input byte).  One worker thread
+ * launches a batch on one stream while it completes the previous batch on the
+ * other, so requests that arrive while a batch runs join the next one.  Every
+ * request gets exactly the result it would get alone (windows are independent).
+ * src and the output buffers must stay valid until gcz_server_wait returns. */
+typedef struct gcz_server gcz_server;
+enum { GCZ_REQ_ZSTD = 0, GCZ_REQ_LZMA2 = 1 };
+
+int gcz_server_create(gcz_ctx *ctx, uint64_t hbm_budget, uint64_t max_batch_bytes, uint32_t max_batch_requests,
+                      gcz_server **out);
+void gcz_server_destroy(gcz_server *server);  /* finishes every submitted request first */
+uint64_t gcz_server_max_batch_bytes(const gcz_server *server);
+/* GCZ_REQ_ZSTD: out_a = gcz_zstd_sequence[cap_a], out_b = uint64_t[num_windows+1] offsets.
+ * GCZ_REQ_LZMA2: out_a = uint32_t[n] packed (or NULL), out_b = uint8_t[num_windows] has-match bytes
+ * (or NULL); search_depth as for the direct calls.  GCZ_ETOOLARGE if n > max batch bytes. */
+int gcz_server_submit(gcz_server *server, int kind, uint32_t search_depth, const uint8_t *src, size_t n, void *out_a,
+                      size_t cap_a, void *out_b, uint64_t *request_id);
+/* Blocks until the request is done (or timeout_s passes: GCZ_EDEVICE) and returns its
+ * status; latency_ms = submit-to-completion time. */
+int gcz_server_wait(gcz_server *server, uint64_t request_id, double timeout_s, double *latency_ms);
+/* Completed requests, their input bytes, batches launched, latency percentiles (ms). */
+int gcz_server_stats(gcz_server *server, uint64_t *completed, uint64_t *bytes, uint64_t *batches, double *p50_ms,
+                     double *p99_ms);
+
 /* ---------------------------------------------------------------- timing */
 
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this

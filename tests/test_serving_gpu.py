@@ -1,0 +1,81 @@
+"""The request loop: requests of mixed kind and size, submitted from several
+threads while batches run, each get exactly the result they get alone."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mixed_stream_equals_alone(ctx):
+    import gcz
+    from gcz import serving
+
+    rng = np.random.default_rng(3)
+    sizes = [int(x) for x in np.exp(rng.uniform(np.log(1), np.log(3 << 20), size=90))] + [0, 1, 65536, 65537]
+    kinds = [serving.ZSTD if rng.random() < 0.8 else serving.LZMA2 for _ in sizes]
+    depths = [int(rng.choice([1, 16, 64])) if k == serving.ZSTD else 32 for k in kinds]
+    datas = [gcz.gen_synthetic(500 + i, s, 8 << 20, tuple(rng.dirichlet([1, 1, 1]))) for i, s in enumerate(sizes)]
+    srv = serving.Server(ctx, hbm_budget=4 * 10**9, max_batch_bytes=16 << 20)
+    reqs = [None] * len(sizes)
+
+    def submitter(idx):
+        for i in idx:
+            reqs[i] = srv.submit(kinds[i], datas[i], depths[i])
+
+    threads = [threading.Thread(target=submitter, args=(range(j, len(sizes), 3),)) for j in range(3)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    results = [srv.wait(r) for r in reqs]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(sizes) and st["status"] == 0
+    assert st["batches"] < len(sizes)  # requests really were batched together
+    for i, res in enumerate(results):
+        if kinds[i] == serving.ZSTD:
+            s, o = ctx.zstd_match_find(datas[i], depths[i])
+            np.testing.assert_array_equal(res[1], o)
+            np.testing.assert_array_equal(res[0], s)
+        else:
+            p, h = ctx.lzma2_match_find(datas[i], 32)
+            np.testing.assert_array_equal(res[0], p)
+            np.testing.assert_array_equal(res[1], h)
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_oversized_request_is_rejected(ctx):
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=1 << 20)
+    assert srv.max_batch_bytes == 1 << 20
+    with pytest.raises(gcz.GczError):
+        srv.submit(serving.ZSTD, np.zeros((1 << 20) + 1, np.uint8))
+    srv.close()
+
+
+def test_caller_buffers_and_has_only_lzma2(ctx):
+    """Caller-owned (reused) output buffers; an LZMA2 request without a packed
+    output returns only the per-window has-match bytes."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=8 << 20)
+    a = np.empty((1 << 18, 4), np.uint32)
+    b = np.zeros(1024, np.uint64)
+    h = np.zeros(1024, np.uint8)
+    for i, n in enumerate([70000, 3 << 20, 5]):
+        data = gcz.gen_synthetic(900 + i, n, 8 << 20)
+        rz = srv.submit(serving.ZSTD, data, 16, out_a=a, out_b=b, cap=a.shape[0])
+        rl = srv.submit(serving.LZMA2, data, 32, out_b=h, packed=False)
+        seqs, off = srv.wait(rz)
+        p, has = srv.wait(rl)
+        s0, o0 = ctx.zstd_match_find(data, 16)
+        np.testing.assert_array_equal(off, o0)
+        np.testing.assert_array_equal(seqs, s0)
+        assert p is None
+        np.testing.assert_array_equal(has, ctx.lzma2_match_find(data, 32)[1])
+    srv.close()
