@@ -146,19 +146,15 @@ def barrier(dist, torch, local):
 
 
 def max_over_ranks(dist, torch, value):
-    if dist is None:
-        return value
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from gcz import shards
+
+    return value if dist is None else shards.max_over_ranks(value)
 
 
 def sum_over_ranks(dist, torch, value):
-    if dist is None:
-        return value
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    from gcz import shards
+
+    return value if dist is None else shards.sum_over_ranks(value)
 
 
 def measured_traffic(workload, n):

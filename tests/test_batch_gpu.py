@@ -108,3 +108,19 @@ def test_autotuner_keeps_results_and_picks_a_config(ctx, tmp_path):
     ctx.set_option("algo", 2)
     ctx.set_option("parse_ctas", 3)
     ctx.set_option("staged", 1)
+
+
+def test_sharded_single_rank_uses_gpu_context(ctx):
+    """Without a process group gcz.shards runs the whole input on this GPU."""
+    import gcz
+    from gcz import shards
+
+    data = gcz.gen_synthetic(71, 3 * 65536 + 5, 8 << 20)
+    s, o = shards.zstd_match_find_sharded(data, 16)
+    s0, o0 = ctx.zstd_match_find(data, 16)
+    np.testing.assert_array_equal(o, o0)
+    np.testing.assert_array_equal(s, s0)
+    p, h = shards.lzma2_match_find_sharded(data, 32)
+    p0, h0 = ctx.lzma2_match_find(data, 32)
+    np.testing.assert_array_equal(p, p0)
+    np.testing.assert_array_equal(h, h0)
