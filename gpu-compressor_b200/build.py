@@ -15,7 +15,8 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "gcz", "libgcz.so")
 
-SOURCES = ["gcz_api.cu", "gcz_sweep.cu", "gcz_zstd.cu", "gcz_zstd2.cu", "gcz_lzma2.cu", "gcz_noalloc.cu", "gcz_gen.cpp"]
+SOURCES = ["gcz_api.cu", "gcz_sweep.cu", "gcz_zstd.cu", "gcz_zstd2.cu", "gcz_lzma2.cu", "gcz_noalloc.cu", "gcz_gen.cpp",
+           "gcz_frames.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]
@@ -32,7 +33,7 @@ def build(force=False, verbose=False):
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= _newest(deps):
         return OUT
     cmd = [NVCC] + ARCH + FLAGS + ["-I", INCLUDE, "-I", CSRC] + [os.path.join(CSRC, s) for s in SOURCES] + [
-        "-o", OUT + ".tmp", "-lpthread"]
+        "-o", OUT + ".tmp", "-lpthread", "-ldl"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "gcz.h"
+#include "gcz_internal.h"
 #include "gcz_kernels.h"
 
 namespace {
@@ -83,6 +84,17 @@ int fail(gcz_ctx *c, int code, const char *fmt, ...) {
     if (c) c->err = buf;
     return code;
 }
+
+}  // namespace
+
+int gcz_internal_fail(gcz_ctx *c, int code, const char *msg) {
+    if (!c) return code;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->err = msg;
+    return code;
+}
+
+namespace {
 
 #define GCZ_CUDA(c, call)                                                                          \
     do {                                                                                           \
@@ -572,7 +584,7 @@ namespace {
 // host once they have arrived.
 template <class Consume>
 int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, uint32_t *packed_out,
-                     uint8_t *has_out, Consume consume) {
+                     uint8_t *has_out, bool copy_packed, Consume consume) {
     const size_t nb = nwin(n);
     int r = GCZ_OK;
     auto finish = [&](Slot &sl) -> int {
@@ -597,12 +609,14 @@ int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, u
                                   static_cast<uint32_t *>(sl.lz_packed.p), static_cast<uint8_t *>(sl.lz_has.p),
                                   sl.st)) != GCZ_OK)
             break;
-        uint32_t *dst = packed_out ? packed_out + sl.off : nullptr;
-        if (!dst) {
-            if ((r = ensure_host(c, sl.h_packed, sb * (size_t)kW * 4)) != GCZ_OK) break;
-            dst = static_cast<uint32_t *>(sl.h_packed.p);
+        if (copy_packed) {  // a has-only call (packed == NULL) copies back one byte per window
+            uint32_t *dst = packed_out ? packed_out + sl.off : nullptr;
+            if (!dst) {
+                if ((r = ensure_host(c, sl.h_packed, sb * (size_t)kW * 4)) != GCZ_OK) break;
+                dst = static_cast<uint32_t *>(sl.h_packed.p);
+            }
+            GCZ_CUDA(c, cudaMemcpyAsync(dst, sl.lz_packed.p, sl.len * 4, cudaMemcpyDeviceToHost, sl.st));
         }
-        GCZ_CUDA(c, cudaMemcpyAsync(dst, sl.lz_packed.p, sl.len * 4, cudaMemcpyDeviceToHost, sl.st));
         if (has_out) GCZ_CUDA(c, cudaMemcpyAsync(has_out + b0, sl.lz_has.p, sb, cudaMemcpyDeviceToHost, sl.st));
         GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
         sl.busy = true;
@@ -623,7 +637,8 @@ extern "C" int gcz_lzma2_match_find(gcz_ctx *c, const uint8_t *src, size_t n, ui
     std::lock_guard<std::mutex> lk(c->mu);
     if (n && !src) return fail(c, GCZ_EINVAL, "null pointer");
     DeviceGuard g(c->device);
-    return lzma_host_slices(c, src, n, search_depth, packed, has_matches, [](size_t, size_t, const uint32_t *) {});
+    return lzma_host_slices(c, src, n, search_depth, packed, has_matches, packed != nullptr,
+                            [](size_t, size_t, const uint32_t *) {});
 }
 
 extern "C" int gcz_lzma2_find_matches(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t max_matches,
@@ -649,7 +664,7 @@ extern "C" int gcz_lzma2_find_matches(gcz_ctx *c, const uint8_t *src, size_t n, 
     zero(match_counts, total_pos);
     zero(match_distances, total_pos * max_matches);
     zero(match_lengths, total_pos * max_matches);
-    return lzma_host_slices(c, src, n, GCZ_LZMA2_SEARCH_DEPTH, nullptr, nullptr,
+    return lzma_host_slices(c, src, n, GCZ_LZMA2_SEARCH_DEPTH, nullptr, nullptr, true,
                             [&](size_t off, size_t len, const uint32_t *pk) {
                                 for (size_t i = 0; i < len; i++) {
                                     const uint32_t v = pk[i];

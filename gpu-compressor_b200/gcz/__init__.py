@@ -144,6 +144,16 @@ class Context:
                                            has.ctypes.data))
         return packed[:n], has[:num_windows(n)]
 
+    def lzma2_triage(self, data, search_depth=LZMA2_SEARCH_DEPTH):
+        """has_matches u8[B] only: the per-window bit the LZMA2 L1+ encoder
+        consumes (compress_lzma2_custom.rs:577); no per-position results cross
+        back to the host."""
+        src = _u8(data)
+        n = src.size
+        has = np.zeros(max(num_windows(n), 1), np.uint8)
+        self._check(L.gcz_lzma2_match_find(self._h, _ptr(src), n, search_depth, None, has.ctypes.data))
+        return has[:num_windows(n)]
+
     def lzma2_match_find_device(self, d_src, n, search_depth, d_packed, d_has, stream=None):
         self._check(L.gcz_lzma2_match_find_device(self._h, d_src, n, search_depth, d_packed, d_has, _stream(stream)))
 
@@ -191,6 +201,20 @@ class Context:
         self._check(L.gcz_lzma2_match_find_batch_device(self._h, d_slab, slab_bytes, d_windows, num_windows,
                                                         search_depth, d_packed, d_has, _stream(stream)))
 
+    # ------------------------------------------------------------ frames
+    def zstd_compress_frames(self, data, level=1, threads=0):
+        """One Zstd frame per 64 KiB window (GPU sequences, libzstd
+        ZSTD_compressSequences on `threads` CPU threads, 0 = all cores):
+        (frames bytes back to back, frame sizes u64[B])."""
+        src = _u8(data)
+        n = src.size
+        out = np.empty(max(int(L.gcz_zstd_frames_bound(n)), 1), np.uint8)
+        sizes = np.zeros(max(num_windows(n), 1), np.uint64)
+        used = ctypes.c_size_t()
+        self._check(L.gcz_zstd_compress_frames(self._h, _ptr(src), n, level, threads, out.ctypes.data, out.size,
+                                               sizes.ctypes.data, ctypes.byref(used)))
+        return out[:used.value], sizes[:num_windows(n)]
+
     # ------------------------------------------------------------ timing
     def profile_start(self):
         self._check(L.gcz_profile_start(self._h))
@@ -219,21 +243,16 @@ def context(device_id=0):
 def compress_chunk_zstd_custom(chunk_data, device_id=0, level=1):
     """compress_chunk_zstd_custom (compress_zstd_custom.rs:47-203): GPU match
     finding per 64 KiB window, then one Zstd frame per window through libzstd's
-    ZSTD_compressSequences.  Returns (frames, sizes)."""
+    ZSTD_compressSequences (gcz_zstd_compress_frames: a pool of CPU coder
+    threads encodes one slice while the GPU matches the next).  Returns
+    (frames, sizes)."""
     data = _u8(chunk_data)
-    depth = search_depth_for_level(level)
-    seqs, offsets = context(device_id).zstd_match_find(data, depth)
-    comp = codecs.SequenceCompressor()
-    frames, sizes = [], []
-    try:
-        for b in range(offsets.size - 1):
-            win = data[b * WINDOW:(b + 1) * WINDOW]
-            f = comp.compress(win, seqs[int(offsets[b]):int(offsets[b + 1])])
-            frames.append(f)
-            sizes.append(len(f))
-    finally:
-        comp.close()
-    return frames, sizes
+    blob, fsizes = context(device_id).zstd_compress_frames(data, level)
+    frames, pos = [], 0
+    for s in fsizes.tolist():
+        frames.append(blob[pos:pos + s].tobytes())
+        pos += s
+    return frames, [len(f) for f in frames]
 
 
 @dataclass

@@ -56,13 +56,23 @@ def read_container(blob):
     return magic, orig, chunk_size, chunks
 
 
-def compress_zstd(data, level=1, device_id=0):
-    """NVZS with one Zstd frame per 64 KiB window (the Zstd L1/L2 path)."""
-    from . import compress_chunk_zstd_custom
+def write_container_frames(magic, orig_size, chunk_size, sizes, blob):
+    """write_container for chunks already laid out back to back in `blob`."""
+    sizes = [int(x) for x in sizes]
+    head = HEADER.pack(magic, orig_size, chunk_size, len(sizes))
+    return head + (struct.pack(f"<{len(sizes)}Q", *sizes) if sizes else b"") + bytes(blob)
+
+
+def compress_zstd(data, level=1, device_id=0, threads=0):
+    """NVZS with one Zstd frame per 64 KiB window (the Zstd L1/L2 path);
+    `threads` CPU coder threads (0 = all cores)."""
+    from . import context
 
     buf = np.frombuffer(memoryview(data).cast("B"), dtype=np.uint8)
-    frames, _ = compress_chunk_zstd_custom(buf, device_id, level) if buf.size else ([], [])
-    return write_container(MAGIC_ZSTD, buf.size, WINDOW, frames)
+    if buf.size == 0:
+        return write_container(MAGIC_ZSTD, 0, WINDOW, [])
+    blob, sizes = context(device_id).zstd_compress_frames(buf, level, threads)
+    return write_container_frames(MAGIC_ZSTD, buf.size, WINDOW, sizes, blob)
 
 
 def compress_lzma2(data, device_id=0, workers=None):
@@ -74,7 +84,7 @@ def compress_lzma2(data, device_id=0, workers=None):
     buf = np.frombuffer(memoryview(data).cast("B"), dtype=np.uint8)
     if buf.size == 0:
         return write_container(MAGIC_LZMA2, 0, WINDOW, [])
-    _, has = context(device_id).lzma2_match_find(buf)
+    has = context(device_id).lzma2_triage(buf)
     nb = num_windows(buf.size)
     workers = workers or min(os.cpu_count() or 1, 8)
 

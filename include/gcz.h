@@ -41,6 +41,8 @@ enum {
     GCZ_ECAPACITY = -4,  /* an output buffer is too small */
     GCZ_EDEVICE = -5,    /* a kernel reported an error status (bounded wait expired) */
     GCZ_ETOOLARGE = -6,  /* input larger than gcz_zstd_match_find_device_noalloc's static scratch */
+    GCZ_EUNAVAILABLE = -7, /* a run-time library the call needs (libzstd) could not be loaded */
+    GCZ_ECODEC = -8,     /* the CPU entropy coder failed */
 };
 
 typedef struct gcz_ctx gcz_ctx;
@@ -157,7 +159,8 @@ int gcz_zstd_match_find_ref_layout_device(gcz_ctx *ctx, const uint8_t *d_input, 
 /* Compact form: packed[q] for every q < n (n entries), and has_matches[b]
  * (num_windows bytes, 0/1) = any(match_counts > 0) over window b -- the one bit
  * encode_single_sub_block consumes (compress_lzma2_custom.rs:577).  Either
- * output may be NULL. */
+ * output may be NULL; with packed == NULL only the has_matches bytes cross
+ * back to the host (the triage call of the LZMA2 L1+ path). */
 int gcz_lzma2_match_find(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t search_depth,
                          uint32_t *packed, uint8_t *has_matches);
 int gcz_lzma2_match_find_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, uint32_t search_depth,
@@ -249,6 +252,22 @@ int gcz_server_stats(gcz_server *server, uint64_t *completed, uint64_t *bytes, u
                      double *p99_ms);
 
 /* ---------------------------------------------------------------- timing */
+
+/* ---------------------------------------------------------------- frames */
+
+/* Zstd L1/L2 frames of a host buffer: compress_chunk_zstd_custom
+ * (compress_zstd_custom.rs:47-203) over the whole input, one Zstd frame per
+ * 64 KiB window, written back to back into `out` in window order with
+ * frame_sizes[b] (num_windows entries) -- the frames and size table an NVZS
+ * container holds (pipeline.rs:163-168,217-225).  The GPU finds the sequences
+ * of one 32 MiB slice while `threads` CPU threads (0 = all cores) run libzstd's
+ * ZSTD_compressSequences on the previous slice, each window exactly as the
+ * reference does it, so the frames equal the reference's byte for byte.
+ * libzstd (>= 1.5) is loaded at run time; GCZ_EUNAVAILABLE without it.
+ * out_capacity >= gcz_zstd_frames_bound(n) always suffices. */
+size_t gcz_zstd_frames_bound(size_t n);
+int gcz_zstd_compress_frames(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t level, uint32_t threads,
+                             uint8_t *out, size_t out_capacity, uint64_t *frame_sizes, size_t *out_size);
 
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this
  * context launches is bracketed by CUDA events on its own launch stream.

@@ -50,3 +50,22 @@ def test_lzma2_raw_paths_decode():
     raw = codecs.lzma2_raw_chunks(data)
     assert raw[0] == 0x01 and raw[65536 + 3] == 0x02 and raw[-1] == 0x00
     assert codecs.lzma2_raw_decompress(raw) == data
+
+
+def test_frames_bound_is_sum_of_compress_bounds():
+    import gcz
+    from gcz import codecs
+
+    zb = codecs.zstd().ZSTD_compressBound
+    for n in [0, 1, 65535, 65536, 65537, 3 * 65536 + 5, 1 << 30]:
+        want = sum(zb(min(65536, n - o)) for o in range(0, n, 65536))
+        assert gcz.L.gcz_zstd_frames_bound(n) == want
+
+
+def test_write_container_frames_matches_write_container():
+    from gcz import formats
+
+    chunks = [b"ab", b"", b"xyz" * 9]
+    assert formats.write_container_frames(formats.MAGIC_ZSTD, 99, 65536, [len(c) for c in chunks],
+                                          b"".join(chunks)) == formats.write_container(formats.MAGIC_ZSTD, 99,
+                                                                                        65536, chunks)

@@ -111,3 +111,17 @@ def test_full_size_1gib_vs_oracle(ctx):
     rng = np.random.default_rng(1)
     lo = int(rng.integers(0, n - 200000))
     check_lzma_packed(data[lo - lo % 65536:lo - lo % 65536 + 131072], packed[lo - lo % 65536:lo - lo % 65536 + 131072])
+
+
+def test_triage_returns_has_matches_only(ctx):
+    """packed == NULL: only the per-window has-match bytes come back, equal to
+    the full call's (and to the oracle's) on windows with and without matches."""
+    import gcz
+
+    data = np.concatenate([gcz.gen_synthetic(81, 5 * 65536 + 9, 128 << 20),
+                           np.arange(65536, dtype=np.uint32).view(np.uint8)[:65536],
+                           np.zeros(3, np.uint8)])
+    has = ctx.lzma2_triage(data)
+    p, h = ctx.lzma2_match_find(data)
+    np.testing.assert_array_equal(has, h)
+    np.testing.assert_array_equal(has, orc.has_matches(orc.lzma_packed(data, 32), data.size))

@@ -96,3 +96,43 @@ def test_gpu_find_matches_then_encode(ctx):
         sub = data[i * 65536:(i + 1) * 65536]
         block = gcz.encode_single_sub_block(sub, md.match_counts_of(i))
         assert codecs.lzma2_raw_decompress(block) == sub.tobytes()
+
+
+@pytest.mark.parametrize("n,level,threads", [(40 * 65536 * 16 + 77, 1, 0), (5 * 65536 + 3, 2, 1), (1, 1, 3)])
+def test_native_frames_equal_serial_libzstd(ctx, n, level, threads):
+    """gcz_zstd_compress_frames (slices over GPU + coder pool) gives, window by
+    window, the frame the serial ZSTD_compressSequences loop gives for the
+    oracle's sequences; the 40 MiB case crosses the 32 MiB slice boundary."""
+    import gcz
+    from gcz import codecs
+
+    data = gcz.gen_synthetic(200 + n % 97, n, 8 << 20)
+    blob, sizes = ctx.zstd_compress_frames(data, level, threads)
+    assert sizes.size == gcz.num_windows(n) and int(sizes.sum()) == blob.size
+    o_seqs, o_off = orc.zstd_sequences(data, gcz.search_depth_for_level(level), threads=16)
+    comp = codecs.SequenceCompressor()
+    pos = 0
+    for b in range(sizes.size):
+        win = data[b * 65536:(b + 1) * 65536]
+        f = blob[pos:pos + int(sizes[b])].tobytes()
+        pos += int(sizes[b])
+        assert f == comp.compress(win, o_seqs[int(o_off[b]):int(o_off[b + 1])]), b
+        if b % 37 == 0:
+            assert codecs.zstd_decompress(f, win.size) == win.tobytes()
+    comp.close()
+
+
+def test_native_frames_empty_and_capacity(ctx):
+    import ctypes
+    import gcz
+
+    blob, sizes = ctx.zstd_compress_frames(np.zeros(0, np.uint8))
+    assert blob.size == 0 and sizes.size == 0
+    data = gcz.gen_synthetic(5, 3 * 65536, 8 << 20)
+    out = np.empty(1000, np.uint8)
+    fs = np.zeros(3, np.uint64)
+    used = ctypes.c_size_t()
+    rc = gcz.L.gcz_zstd_compress_frames(ctx.handle, data.ctypes.data, data.size, 1, 2, out.ctypes.data, out.size,
+                                        fs.ctypes.data, ctypes.byref(used))
+    assert rc == -4 and used.value == 0  # GCZ_ECAPACITY
+    assert b"too small" in gcz.L.gcz_last_error(ctx.handle)
