@@ -16,7 +16,7 @@ INCLUDE = os.path.join(ROOT, "include")
 OUT = os.path.join(HERE, "gcz", "libgcz.so")
 
 SOURCES = ["gcz_api.cu", "gcz_sweep.cu", "gcz_zstd.cu", "gcz_zstd2.cu", "gcz_lzma2.cu", "gcz_noalloc.cu", "gcz_gen.cpp",
-           "gcz_frames.cpp"]
+           "gcz_frames.cpp", "gcz_zenc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr"]

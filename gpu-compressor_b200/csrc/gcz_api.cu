@@ -37,16 +37,18 @@ struct EventPair {
 // Device scratch of one match-find step.
 struct Scratch {
     DevBuf packed, counts, cand, seg;
+    DevBuf zslots, zovs, zaux;  // Zstd entropy stage: frame slots, offset codes, per-window words
 };
 
 // One stage of the host-buffer pipeline: its own stream, input, scratch and
 // outputs, so that the copies of one slice overlap the kernels of another.
 struct Slot {
     Scratch sc;
-    DevBuf in, offsets, seqs, lz_packed, lz_has;
-    HostBuf h_off, h_packed;
+    DevBuf in, offsets, seqs, lz_packed, lz_has, frames, foff;
+    HostBuf h_off, h_packed, h_foff;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev = nullptr;      // the slice's kernels (and small copies) are done
+    cudaEvent_t ev_out = nullptr;  // the slice's results have left its device buffers
     bool busy = false;
     size_t b0 = 0, sb = 0, off = 0, len = 0;
 };
@@ -57,6 +59,7 @@ struct gcz_ctx {
     int device = 0;
     int num_sms = 148;
     cudaStream_t stream = nullptr;
+    cudaStream_t out_stream = nullptr;  // copies of results back to the host (host-buffer pipeline)
     std::mutex mu;
     std::string err;
     uint32_t *d_status = nullptr;
@@ -177,7 +180,8 @@ int read_status(gcz_ctx *c, cudaStream_t st) {
     if (h) {
         GCZ_CUDA(c, cudaMemsetAsync(c->d_status, 0, 4, st));
         GCZ_CUDA(c, cudaStreamSynchronize(st));
-        if (h & 2u) return fail(c, GCZ_ECAPACITY, "sequence output capacity exceeded (device status %u)", h);
+        if (h & 2u) return fail(c, GCZ_ECAPACITY, "output capacity exceeded (device status %u)", h);
+        if (h & 4u) return fail(c, GCZ_EINVAL, "sequences do not describe their windows (device status %u)", h);
         return fail(c, GCZ_EDEVICE, "kernel reported status %u (bounded wait expired)", h);
     }
     return GCZ_OK;
@@ -263,6 +267,37 @@ int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st)
     return GCZ_OK;
 }
 
+// Zstd frames of windows [0, nwin(n)) from their ZSTD_Sequence records:
+// frames back to back in d_out, frame offsets (nwin+1) in d_frame_offsets.
+int zenc_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, const void *d_seqs,
+              const uint64_t *d_seq_offsets, uint8_t *d_out, uint64_t out_capacity, uint64_t *d_frame_offsets,
+              cudaStream_t st) {
+    const size_t nb = nwin(n);
+    int r;
+    if ((r = ensure_dev(c, sc.zslots, nb * (size_t)gcz::kZencSlot)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sc.zovs, nb * (size_t)gcz::kZencMaxSeqs * 4)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sc.zaux, nb * 12 + 64)) != GCZ_OK) return r;
+    gcz::ZencLaunch l{};
+    l.src = d_src;
+    l.n = n;
+    l.window = kW;
+    l.num_windows = (uint32_t)nb;
+    l.seqs = d_seqs;
+    l.seq_offsets = d_seq_offsets;
+    l.slots = static_cast<uint8_t *>(sc.zslots.p);
+    l.ovs = static_cast<uint32_t *>(sc.zovs.p);
+    l.sec_off = static_cast<uint32_t *>(sc.zaux.p);
+    l.fsize = l.sec_off + nb;
+    l.raw = reinterpret_cast<uint8_t *>(l.fsize + nb);
+    l.status = c->d_status;
+    l.num_sms = c->num_sms;
+    GCZ_CUDA(c, gcz::launch_zenc(l, st));
+    GCZ_CUDA(c, gcz::launch_scan_counts(l.fsize, (uint32_t)nb, d_frame_offsets, st));
+    GCZ_CUDA(c, gcz::launch_zenc_compact(l, d_frame_offsets, d_out, out_capacity, st));
+    c->all_launches += 4;
+    return GCZ_OK;
+}
+
 int lzma_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, uint32_t depth, uint32_t *d_packed,
                      uint8_t *d_has, cudaStream_t st) {
     const size_t nb = nwin(n);
@@ -305,10 +340,12 @@ extern "C" int gcz_create(int device_id, gcz_ctx **out) {
     }
     c->num_sms = prop.multiProcessorCount;
     bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&c->d_status, 16) == cudaSuccess && cudaMemset(c->d_status, 0, 16) == cudaSuccess;
     for (Slot &sl : c->slots)
         ok = ok && cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) == cudaSuccess &&
-             cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess;
+             cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&sl.ev_out, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
         if (c->stream) cudaStreamDestroy(c->stream);
@@ -325,19 +362,24 @@ extern "C" void gcz_destroy(gcz_ctx *c) {
         DeviceGuard g(c->device);
         cudaStreamSynchronize(c->stream);
         auto free_scratch = [](Scratch &x) {
-            for (DevBuf *b : {&x.packed, &x.counts, &x.cand, &x.seg})
+            for (DevBuf *b : {&x.packed, &x.counts, &x.cand, &x.seg, &x.zslots, &x.zovs, &x.zaux})
                 if (b->p) cudaFree(b->p);
         };
         free_scratch(c->sc);
         for (Slot &sl : c->slots) {
             if (sl.st) cudaStreamSynchronize(sl.st);
             free_scratch(sl.sc);
-            for (DevBuf *b : {&sl.in, &sl.offsets, &sl.seqs, &sl.lz_packed, &sl.lz_has})
+            for (DevBuf *b : {&sl.in, &sl.offsets, &sl.seqs, &sl.lz_packed, &sl.lz_has, &sl.frames, &sl.foff})
                 if (b->p) cudaFree(b->p);
-            for (HostBuf *b : {&sl.h_off, &sl.h_packed})
+            for (HostBuf *b : {&sl.h_off, &sl.h_packed, &sl.h_foff})
                 if (b->p) cudaFreeHost(b->p);
             if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.ev_out) cudaEventDestroy(sl.ev_out);
             if (sl.st) cudaStreamDestroy(sl.st);
+        }
+        if (c->out_stream) {
+            cudaStreamSynchronize(c->out_stream);
+            cudaStreamDestroy(c->out_stream);
         }
         for (auto &e : c->events) {
             cudaEventDestroy(e.a);
@@ -442,7 +484,9 @@ int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, 
     sl.busy = false;
     if (done + total > cap)
         return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)(done + total), cap);
-    if (total) GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, sl.seqs.p, total * 16, cudaMemcpyDeviceToHost, sl.st));
+    // On the copy-out stream, so that the slot's next copy-in does not queue behind it.
+    if (total) GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, sl.seqs.p, total * 16, cudaMemcpyDeviceToHost, c->out_stream));
+    GCZ_CUDA(c, cudaEventRecord(sl.ev_out, c->out_stream));
     for (size_t i = 1; i <= sl.sb; i++) offsets[sl.b0 + i] = done + ho[i];
     done += total;
     return GCZ_OK;
@@ -450,6 +494,7 @@ int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, 
 
 int drain_slots(gcz_ctx *c) {
     for (Slot &sl : c->slots) GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+    GCZ_CUDA(c, cudaStreamSynchronize(c->out_stream));
     return read_status(c, c->stream);
 }
 }  // namespace
@@ -481,6 +526,7 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
         if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(slice_cap, 1) * 16)) != GCZ_OK) break;
         if ((r = ensure_host(c, sl.h_off, (sb + 1) * 8)) != GCZ_OK) break;
         GCZ_CUDA(c, cudaMemcpyAsync(sl.in.p, src + sl.off, sl.len, cudaMemcpyHostToDevice, sl.st));
+        GCZ_CUDA(c, cudaStreamWaitEvent(sl.st, sl.ev_out, 0));  // sl.seqs free again
         if ((r = zstd_device_core(c, sl.sc, static_cast<const uint8_t *>(sl.in.p), sl.len, search_depth, sl.seqs.p,
                                   slice_cap, static_cast<uint64_t *>(sl.offsets.p), sl.st)) != GCZ_OK)
             break;
@@ -494,6 +540,91 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
     if (r == GCZ_OK && last.busy) r = zstd_finish_slot(c, last, seqs, seq_capacity, offsets, done);
     for (Slot &sl : c->slots) sl.busy = false;
     const int r2 = drain_slots(c);
+    return r != GCZ_OK ? r : r2;
+}
+
+extern "C" int gcz_zstd_encode_frames_device(gcz_ctx *c, const uint8_t *d_src, size_t n,
+                                             const gcz_zstd_sequence *d_seqs, const uint64_t *d_seq_offsets,
+                                             uint8_t *d_out, size_t out_capacity, uint64_t *d_frame_offsets,
+                                             void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!d_src || !d_seqs || !d_seq_offsets || !d_out)) || !d_frame_offsets)
+        return fail(c, GCZ_EINVAL, "null pointer");
+    if (nwin(n) > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "input too large");
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    if (n == 0) {
+        GCZ_CUDA(c, cudaMemsetAsync(d_frame_offsets, 0, 8, st));
+        return GCZ_OK;
+    }
+    return zenc_core(c, c->sc, d_src, n, d_seqs, d_seq_offsets, d_out, out_capacity, d_frame_offsets, st);
+}
+
+// Host bytes to Zstd frames entirely on the GPU: slices alternate between the
+// two pipeline slots; slice k's copy-in, match finding and entropy stage run
+// while slice k-1's frames are copied out.
+extern "C" int gcz_zstd_compress_frames_gpu(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t level, uint8_t *out,
+                                            size_t out_capacity, uint64_t *frame_sizes, size_t *out_size) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!src || !out || !frame_sizes)) || !out_size) return fail(c, GCZ_EINVAL, "null pointer");
+    *out_size = 0;
+    DeviceGuard g(c->device);
+    const uint32_t depth = gcz_zstd_search_depth_for_level(level);
+    const size_t nb = nwin(n);
+    size_t written = 0;
+    int r = GCZ_OK;
+    auto finish = [&](Slot &sl) -> int {
+        GCZ_CUDA(c, cudaEventSynchronize(sl.ev));
+        sl.busy = false;
+        const uint64_t *ho = static_cast<const uint64_t *>(sl.h_foff.p);
+        const uint64_t total = ho[sl.sb];
+        if (written + total > out_capacity)
+            return fail(c, GCZ_ECAPACITY, "frames need %llu bytes, capacity %zu",
+                        (unsigned long long)(written + total), out_capacity);
+        if (total)
+            GCZ_CUDA(c, cudaMemcpyAsync(out + written, sl.frames.p, total, cudaMemcpyDeviceToHost, c->out_stream));
+        GCZ_CUDA(c, cudaEventRecord(sl.ev_out, c->out_stream));
+        for (size_t i = 0; i < sl.sb; ++i) frame_sizes[sl.b0 + i] = ho[i + 1] - ho[i];
+        written += total;
+        return GCZ_OK;
+    };
+    size_t k = 0;
+    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+        Slot &sl = c->slots[k & 1];
+        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sl.b0 = b0;
+        sl.sb = sb;
+        sl.off = b0 * (size_t)kW;
+        sl.len = std::min(n - sl.off, sb * (size_t)kW);
+        const size_t slice_cap = gcz_zstd_max_sequences(sl.len);
+        const size_t fbound = gcz_zstd_frames_bound(sl.len);
+        if ((r = ensure_dev(c, sl.in, sb * (size_t)kW + 64)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.offsets, (sb + 1) * 8)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(slice_cap, 1) * 16)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.frames, fbound)) != GCZ_OK) break;
+        if ((r = ensure_dev(c, sl.foff, (sb + 1) * 8)) != GCZ_OK) break;
+        if ((r = ensure_host(c, sl.h_foff, (sb + 1) * 8)) != GCZ_OK) break;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.in.p, src + sl.off, sl.len, cudaMemcpyHostToDevice, sl.st));
+        const uint8_t *d_in = static_cast<const uint8_t *>(sl.in.p);
+        uint64_t *d_off = static_cast<uint64_t *>(sl.offsets.p);
+        if ((r = zstd_device_core(c, sl.sc, d_in, sl.len, depth, sl.seqs.p, slice_cap, d_off, sl.st)) != GCZ_OK) break;
+        GCZ_CUDA(c, cudaStreamWaitEvent(sl.st, sl.ev_out, 0));  // sl.frames free again
+        if ((r = zenc_core(c, sl.sc, d_in, sl.len, sl.seqs.p, d_off, static_cast<uint8_t *>(sl.frames.p), fbound,
+                           static_cast<uint64_t *>(sl.foff.p), sl.st)) != GCZ_OK)
+            break;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_foff.p, sl.foff.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+        GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
+        sl.busy = true;
+        Slot &prev = c->slots[(k + 1) & 1];
+        if (prev.busy) r = finish(prev);
+    }
+    Slot &last = c->slots[(k + 1) & 1];
+    if (r == GCZ_OK && last.busy) r = finish(last);
+    for (Slot &sl : c->slots) sl.busy = false;
+    const int r2 = drain_slots(c);
+    if (r == GCZ_OK && r2 == GCZ_OK) *out_size = written;
     return r != GCZ_OK ? r : r2;
 }
 

@@ -81,6 +81,28 @@ cudaError_t launch_zstd_literals(const uint8_t *src, uint64_t n, uint32_t window
                                  const uint32_t *ref_seqs, const uint32_t *seq_counts, uint32_t max_seqs, uint8_t *lits,
                                  int num_sms, cudaStream_t st);
 
+// Zstd entropy stage (gcz_zenc.cu): frames from ZSTD_Sequence records.
+constexpr uint32_t kZencSlot = 65536 + 1024;  // per-window frame slot bytes
+constexpr uint32_t kZencMaxSeqs = 21845;      // sequences per window (chunk_size / 3)
+struct ZencLaunch {
+    const uint8_t *src;           // windows at b * window
+    uint64_t n;
+    uint32_t window;
+    uint32_t num_windows;
+    const void *seqs;             // ZSTD_Sequence records (16 B)
+    const uint64_t *seq_offsets;  // num_windows + 1
+    uint8_t *slots;               // num_windows * kZencSlot
+    uint32_t *ovs;                // num_windows * kZencMaxSeqs
+    uint32_t *sec_off;            // num_windows
+    uint32_t *fsize;              // num_windows
+    uint8_t *raw;                 // num_windows
+    uint32_t *status;
+    int num_sms;
+};
+cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st);
+cudaError_t launch_zenc_compact(const ZencLaunch &l, const uint64_t *frame_offsets, uint8_t *out, uint64_t capacity,
+                                cudaStream_t st);
+
 cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st);
 cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaStream_t st);
 cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t window, uint32_t num_windows,

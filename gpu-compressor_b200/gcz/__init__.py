@@ -215,6 +215,23 @@ class Context:
                                                sizes.ctypes.data, ctypes.byref(used)))
         return out[:used.value], sizes[:num_windows(n)]
 
+    def zstd_compress_frames_gpu(self, data, level=1):
+        """One Zstd frame per 64 KiB window, encoded on the GPU (raw literals,
+        predefined FSE tables): (frames back to back, frame sizes u64[B])."""
+        src = _u8(data)
+        n = src.size
+        out = np.empty(max(int(L.gcz_zstd_frames_bound(n)), 1), np.uint8)
+        sizes = np.zeros(max(num_windows(n), 1), np.uint64)
+        used = ctypes.c_size_t()
+        self._check(L.gcz_zstd_compress_frames_gpu(self._h, _ptr(src), n, level, out.ctypes.data, out.size,
+                                                   sizes.ctypes.data, ctypes.byref(used)))
+        return out[:used.value], sizes[:num_windows(n)]
+
+    def zstd_encode_frames_device(self, d_src, n, d_seqs, d_seq_offsets, d_out, out_capacity, d_frame_offsets,
+                                  stream=None):
+        self._check(L.gcz_zstd_encode_frames_device(self._h, d_src, n, d_seqs, d_seq_offsets, d_out, out_capacity,
+                                                    d_frame_offsets, _stream(stream)))
+
     # ------------------------------------------------------------ timing
     def profile_start(self):
         self._check(L.gcz_profile_start(self._h))

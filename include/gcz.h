@@ -269,6 +269,30 @@ size_t gcz_zstd_frames_bound(size_t n);
 int gcz_zstd_compress_frames(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t level, uint32_t threads,
                              uint8_t *out, size_t out_capacity, uint64_t *frame_sizes, size_t *out_size);
 
+/* Zstd frames built on the GPU (no reference counterpart: the reference's
+ * GPU block encoder, zstd_compress.cu:756-1038, is unused and its output is
+ * not decodable).  Each 64 KiB window becomes one frame with a single block:
+ * raw literals and sequences FSE-coded with the format's predefined
+ * distributions (RFC 8878), repeat offsets used where they apply, or a raw
+ * block when that is smaller.  Every frame decodes with stock libzstd to its
+ * window.  The frames differ from libzstd's (no Huffman literals, no tuned
+ * tables), so the ratio is somewhat higher than gcz_zstd_compress_frames'.
+ *
+ * gcz_zstd_compress_frames_gpu: host bytes in, frames back to back in `out`
+ * (out_capacity >= gcz_zstd_frames_bound(n) always suffices) with
+ * frame_sizes[num_windows]; copy-in, match finding, encoding and copy-out of
+ * 64 MiB slices overlap on two streams.
+ * gcz_zstd_encode_frames_device: the entropy stage alone, on device memory,
+ * from the output of gcz_zstd_match_find_device (records + per-window
+ * offsets): frames back to back in d_out, byte offsets of the frames in
+ * d_frame_offsets[num_windows + 1].  Sequences that do not describe their
+ * window give GCZ_EINVAL at the next synchronising call (gcz_sync). */
+int gcz_zstd_compress_frames_gpu(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t level, uint8_t *out,
+                                 size_t out_capacity, uint64_t *frame_sizes, size_t *out_size);
+int gcz_zstd_encode_frames_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, const gcz_zstd_sequence *d_seqs,
+                                  const uint64_t *d_seq_offsets, uint8_t *d_out, size_t out_capacity,
+                                  uint64_t *d_frame_offsets, void *stream);
+
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this
  * context launches is bracketed by CUDA events on its own launch stream.
  * gcz_profile_stop synchronises those events and returns the summed device

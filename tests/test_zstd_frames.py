@@ -1,0 +1,153 @@
+"""GPU Zstd entropy stage.  CPU part: the test-side restatement of the frame
+encoder (zstd_frames_ref) produces frames stock libzstd decodes, on the
+oracle's sequences.  GPU part: the GPU frames equal the restatement's byte for
+byte and decode with stock libzstd, through the host and the device calls."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import cases
+import zstd_frames_ref as zr
+from oracle import oracle as orc
+
+W = 65536
+
+INPUTS = [
+    {"kind": "synthetic", "n": 3 * W + 999, "seed": 41},
+    {"kind": "text", "n": 70000, "seed": 42},
+    {"kind": "zeros", "n": 100000},
+    {"kind": "random", "n": 70000, "seed": 3},
+]
+
+
+def _build(spec):
+    if spec["kind"] == "zeros":
+        return np.zeros(spec["n"], np.uint8)
+    if spec["kind"] == "random":
+        return np.frombuffer(np.random.default_rng(spec["seed"]).bytes(spec["n"]), np.uint8).copy()
+    return cases.build(spec)
+
+
+def _ref_frames(data, depth=16):
+    seqs, off = orc.zstd_sequences(data, depth)
+    out = []
+    for b in range(off.size - 1):
+        s = seqs[int(off[b]):int(off[b + 1])]
+        out.append(zr.encode_frame(data[b * W:(b + 1) * W].tobytes(), [(x[0], x[1], x[2]) for x in s]))
+    return out
+
+
+@pytest.mark.parametrize("spec", INPUTS + [{"kind": "synthetic", "n": n, "seed": 7} for n in (1, 5, 255, 256, 257)],
+                         ids=lambda s: f"{s['kind']}-{s['n']}")
+def test_reference_frames_decode_with_libzstd(spec):
+    from gcz import codecs
+
+    data = _build(spec)
+    for b, f in enumerate(_ref_frames(data)):
+        win = data[b * W:(b + 1) * W]
+        assert codecs.zstd_decompress(f, win.size) == win.tobytes()
+
+
+def _split(blob, sizes):
+    out, pos = [], 0
+    for s in sizes.tolist():
+        out.append(blob[pos:pos + s].tobytes())
+        pos += s
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spec", INPUTS + [{"kind": "synthetic", "n": n, "seed": 7} for n in (1, 5, 255, 256, 257)],
+                         ids=lambda s: f"{s['kind']}-{s['n']}")
+def test_gpu_frames_equal_reference_frames(ctx, spec):
+    data = _build(spec)
+    blob, sizes = ctx.zstd_compress_frames_gpu(data, 1)
+    assert _split(blob, sizes) == _ref_frames(data)
+
+
+@pytest.mark.gpu
+def test_gpu_frames_large_decode_and_level2(ctx):
+    """70 MiB + ragged tail: more than one 64 MiB pipeline slice; every frame
+    decodes; level 2 gives the same bytes as level 1."""
+    import gcz
+    from gcz import codecs
+
+    n = 70 * (1 << 20) + 4321
+    data = gcz.gen_synthetic(17, n, 8 << 20)
+    blob, sizes = ctx.zstd_compress_frames_gpu(data, 1)
+    frames = _split(blob, sizes)
+    assert len(frames) == gcz.num_windows(n)
+    for b in range(0, len(frames), 7):
+        win = data[b * W:(b + 1) * W]
+        assert codecs.zstd_decompress(frames[b], win.size) == win.tobytes()
+    assert 0.3 < blob.size / n < 0.9
+    blob2, sizes2 = ctx.zstd_compress_frames_gpu(data, 2)
+    assert np.array_equal(sizes, sizes2) and np.array_equal(blob, blob2)
+    # a spot check of full equality against the restatement
+    sub = data[:4 * W]
+    assert frames[:4] == _ref_frames(sub)
+
+
+@pytest.mark.gpu
+def test_device_entropy_stage_on_oracle_sequences(ctx):
+    import torch
+    import gcz
+
+    data = gcz.gen_synthetic(23, 5 * W + 77, 8 << 20)
+    seqs, off = orc.zstd_sequences(data, 16)
+    d_src = torch.from_numpy(data).cuda()
+    d_seqs = torch.from_numpy(seqs.astype(np.int32).reshape(-1, 4)).cuda()
+    d_off = torch.from_numpy(off.astype(np.int64)).cuda()
+    cap = int(gcz.L.gcz_zstd_frames_bound(data.size))
+    d_out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    nb = gcz.num_windows(data.size)
+    d_foff = torch.empty(nb + 1, dtype=torch.int64, device="cuda")
+    for _ in range(2):  # second call reuses the scratch
+        ctx.zstd_encode_frames_device(d_src.data_ptr(), data.size, d_seqs.data_ptr(), d_off.data_ptr(),
+                                      d_out.data_ptr(), cap, d_foff.data_ptr(), 0)
+        ctx.sync(0)
+        foff = d_foff.cpu().numpy().astype(np.uint64)
+        blob = d_out[:int(foff[-1])].cpu().numpy()
+        assert _split(blob, np.diff(foff)) == _ref_frames(data)
+
+
+@pytest.mark.gpu
+def test_device_entropy_stage_rejects_bad_sequences(ctx):
+    """An offset reaching before the window start: the kernel's own check turns
+    it into a raw frame and an error status, reported as GCZ_EINVAL."""
+    import torch
+    import gcz
+
+    data = gcz.gen_synthetic(24, W, 8 << 20)
+    seqs = np.array([[5000, 10, 8, 0]], np.int32)  # match at position 10 with offset 5000
+    off = np.array([0, 1], np.int64)
+    d_src = torch.from_numpy(data).cuda()
+    d_seqs = torch.from_numpy(seqs).cuda()
+    d_off = torch.from_numpy(off).cuda()
+    cap = int(gcz.L.gcz_zstd_frames_bound(W))
+    d_out = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    d_foff = torch.empty(2, dtype=torch.int64, device="cuda")
+    ctx.zstd_encode_frames_device(d_src.data_ptr(), W, d_seqs.data_ptr(), d_off.data_ptr(), d_out.data_ptr(), cap,
+                                  d_foff.data_ptr(), 0)
+    with pytest.raises(gcz.GczError) as e:
+        ctx.sync(0)
+    assert e.value.code == -1
+    # the context stays usable
+    blob, sizes = ctx.zstd_compress_frames_gpu(data, 1)
+    assert _split(blob, sizes) == _ref_frames(data)
+
+
+@pytest.mark.gpu
+def test_gpu_frames_empty_and_capacity(ctx):
+    import gcz
+
+    blob, sizes = ctx.zstd_compress_frames_gpu(np.zeros(0, np.uint8))
+    assert blob.size == 0 and sizes.size == 0
+    data = gcz.gen_synthetic(5, 3 * W, 8 << 20)
+    out = np.empty(1000, np.uint8)
+    fs = np.zeros(3, np.uint64)
+    used = ctypes.c_size_t()
+    rc = gcz.L.gcz_zstd_compress_frames_gpu(ctx.handle, data.ctypes.data, data.size, 1, out.ctypes.data, out.size,
+                                            fs.ctypes.data, ctypes.byref(used))
+    assert rc == -4 and used.value == 0
