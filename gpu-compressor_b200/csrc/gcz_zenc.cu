@@ -5,7 +5,8 @@
 // Frame layout (RFC 8878): magic, a single-segment frame header with the
 // content size, and one block.  The block is a compressed block when that is
 // smaller than the window, else a raw block.  A compressed block holds
-//   - a Raw_Literals_Block with every literal byte of the window, in order;
+//   - the window's literal bytes, in order, as the smallest of a raw, an RLE
+//     or a Huffman-coded literals block;
 //   - a sequences section in Predefined_Mode for literal lengths, offsets and
 //     match lengths (the format's default distributions, so no table is
 //     transmitted), whose bitstream is written by an FSE (tANS) encoder
@@ -16,8 +17,9 @@
 // of the three repeat offsets the decoder holds at that point.
 //
 // Kernels, per window:
-//   zenc_literals_kernel   (one CTA):    frame header, literal section
-//   zenc_sequences_kernel  (one thread): repeat-code pass, FSE chains, bitstream,
+//   zenc_literals_kernel   (one CTA):    frame header, literal section (raw, RLE
+//                                        or Huffman-coded)
+//   zenc_sequences_kernel  (one warp):   repeat-code pass, FSE chains, bitstream,
 //                                        block header, frame size
 //   zenc_compact_kernel    (one CTA):    frames back to back at scanned offsets
 // Frames are built in per-window slots of kZencSlot bytes first, because a
@@ -228,8 +230,269 @@ __device__ __forceinline__ void write_block_header(uint8_t *p, uint32_t type, ui
 }
 
 // ---------------------------------------------------------------- literals
+// The literal section is the smallest of: raw; RLE (one distinct byte);
+// Huffman-coded (RFC 8878 4.2), one stream below 1024 literals, else four.
+// The Huffman code: two-queue construction over the present bytes (leaves
+// sorted by count, then byte value; a leaf wins ties), lengths limited to 11
+// bits by moving pairs of leaves up the tree (which keeps the code complete),
+// the longest codes to the least frequent bytes, canonical code values (the
+// longest codes take the smallest values, ties by byte value).  Weights are
+// sent directly when there are at most 128 of them, else FSE-compressed with
+// accuracy 6: counts normalised by floor(c * 64 / N) (at least 1), the
+// largest absorbing the remainder; two interleaved states; the state of the
+// second-to-last weight is chosen with at least one update bit, so that the
+// decoder's last update runs past the stream start and decoding ends there.
+constexpr uint32_t kHufMaxBits = 11;
+
+struct HufSmem {
+    uint32_t count[256];
+    uint32_t node[511];   // node weights, leaves first
+    uint16_t leaf[256];   // present bytes by ascending (count, byte)
+    uint16_t parent[511];
+    uint8_t depth[511];
+    uint8_t len[256];
+    uint16_t code[256];
+    uint8_t tree[132];    // Huffman_Tree_Description
+    uint8_t wts[256];     // transmitted weights
+    uint8_t st[256];      // FSE states of the weights
+    uint8_t fsym[64], fnb[64], fbase[64];
+    uint8_t fenc[12 * 64];
+    uint32_t seg_bits[4];
+    uint32_t tbits[kLitThreads];  // bits of each thread's run of literals
+    uint32_t nsym, tree_bytes, huf_ok, mode, nstreams, seg;
+    uint32_t stream_off[4], stream_bytes[4];
+};
+constexpr uint32_t kLitSmem = kMaxWindow + sizeof(HufSmem);
+
+// Bits into a byte buffer in shared memory, LSB first.
+struct SmemBits {
+    uint8_t *p;
+    uint32_t cap, pos, nbits;
+    uint64_t acc;
+    bool ovf;
+    __device__ void add(uint32_t v, uint32_t nb) {
+        acc |= static_cast<uint64_t>(v) << nbits;
+        nbits += nb;
+        while (nbits >= 8u) {
+            if (pos < cap) p[pos] = static_cast<uint8_t>(acc);
+            else ovf = true;
+            ++pos;
+            acc >>= 8;
+            nbits -= 8u;
+        }
+    }
+    __device__ void flush() {  // pad the last partial byte with zeros
+        if (nbits) add(0u, 8u - nbits);
+    }
+    __device__ void close() {  // end marker, then pad
+        add(1u, 1u);
+        flush();
+    }
+};
+
+// FSE-compressed weights H.wts[0..N) into H.tree + 1; returns its size, or 0.
+__device__ uint32_t huf_fse_weights(HufSmem &H, uint32_t N) {
+    uint32_t cw[12] = {0};
+    for (uint32_t i = 0; i < N; ++i) cw[H.wts[i]]++;
+    uint32_t distinct = 0;
+    for (uint32_t s2 = 0; s2 < 12; ++s2) distinct += cw[s2] ? 1u : 0u;
+    if (distinct < 2) return 0;
+    int norm[12];
+    int sum = 0, big = 0;
+    for (uint32_t s2 = 0; s2 < 12; ++s2) {
+        norm[s2] = cw[s2] ? max(1, static_cast<int>(cw[s2] * 64u / N)) : 0;
+        sum += norm[s2];
+        if (norm[s2] > norm[big]) big = static_cast<int>(s2);
+    }
+    norm[big] += 64 - sum;
+    if (norm[big] <= 0) return 0;
+    // decoder table (no "less than 1" entries, so no high threshold) and encoder map
+    uint32_t pos = 0;
+    for (uint32_t s2 = 0; s2 < 12; ++s2)
+        for (int c = 0; c < norm[s2]; ++c) {
+            H.fsym[pos] = static_cast<uint8_t>(s2);
+            pos = (pos + 43u) & 63u;  // step (64 >> 1) + (64 >> 3) + 3
+        }
+    uint32_t nxt[12];
+    for (uint32_t s2 = 0; s2 < 12; ++s2) nxt[s2] = static_cast<uint32_t>(norm[s2]);
+    for (uint32_t u = 0; u < 64; ++u) {
+        const uint32_t x = nxt[H.fsym[u]]++;
+        const uint32_t nb = 6u - highbit(x);
+        H.fnb[u] = static_cast<uint8_t>(nb);
+        H.fbase[u] = static_cast<uint8_t>((x << nb) - 64u);
+        for (uint32_t v = H.fbase[u]; v < H.fbase[u] + (1u << nb); ++v) H.fenc[H.fsym[u] * 64u + v] = static_cast<uint8_t>(u);
+    }
+    // table description (RFC 8878 4.1.1)
+    SmemBits wr{H.tree + 1, 127u, 0u, 0u, 0ull, false};
+    wr.add(1u, 4u);  // accuracy 6
+    int remaining = 65, threshold = 64;
+    uint32_t nb = 7;
+    int lastw = 11;
+    while (norm[lastw] == 0) --lastw;
+    for (int s2 = 0; s2 <= lastw; ++s2) {
+        const int v = norm[s2] + 1, mx = (2 * threshold - 1) - remaining;
+        if (v < mx) wr.add(static_cast<uint32_t>(v), nb - 1u);
+        else if (v < threshold) wr.add(static_cast<uint32_t>(v), nb);
+        else wr.add(static_cast<uint32_t>(v + mx), nb);
+        remaining -= norm[s2];
+        while (remaining < threshold) {
+            --nb;
+            threshold >>= 1;
+        }
+        if (norm[s2] == 0) {
+            int z = 0;
+            while (s2 + 1 + z < lastw && norm[s2 + 1 + z] == 0) ++z;
+            s2 += z;
+            for (; z >= 3; z -= 3) wr.add(3u, 2u);
+            wr.add(static_cast<uint32_t>(z), 2u);
+        }
+    }
+    wr.flush();
+    // states: the last two weights pick their states, the rest follow the chain
+    const uint32_t w1 = H.wts[N - 1], w2 = H.wts[N - 2];
+    uint32_t s_last = 64, s_prev = 64;
+    for (uint32_t u = 0; u < 64; ++u) {
+        if (s_last == 64 && H.fsym[u] == w1) s_last = u;
+        if (s_prev == 64 && H.fsym[u] == w2 && H.fnb[u] >= 1u) s_prev = u;
+    }
+    if (s_prev == 64) return 0;
+    H.st[N - 1] = static_cast<uint8_t>(s_last);
+    H.st[N - 2] = static_cast<uint8_t>(s_prev);
+    for (int i = static_cast<int>(N) - 3; i >= 0; --i) H.st[i] = H.fenc[H.wts[i] * 64u + H.st[i + 2]];
+    SmemBits bs{H.tree + 1 + wr.pos, 127u > wr.pos ? 127u - wr.pos : 0u, 0u, 0u, 0ull, false};
+    for (int i = static_cast<int>(N) - 3; i >= 0; --i) {
+        const uint32_t sti = H.st[i];
+        bs.add(H.st[i + 2] - H.fbase[sti], H.fnb[sti]);
+    }
+    bs.add(H.st[1], 6u);
+    bs.add(H.st[0], 6u);
+    bs.close();
+    if (wr.ovf || bs.ovf || wr.pos + bs.pos > 127u) return 0;
+    return wr.pos + bs.pos;
+}
+
+// Thread 0: code lengths, canonical codes and the tree description from
+// H.count / H.leaf (H.nsym >= 2 present bytes).  Returns 1 when usable.
+__device__ uint32_t huf_plan(HufSmem &H) {
+    const uint32_t n = H.nsym;
+    for (uint32_t k = 0; k < n; ++k) H.node[k] = H.count[H.leaf[k]];
+    uint32_t li = 0, ii = n, nxt = n;
+    while (nxt < 2u * n - 1u) {
+        uint32_t pick[2];
+        for (uint32_t t = 0; t < 2; ++t) {
+            if (li < n && (ii >= nxt || H.node[li] <= H.node[ii])) pick[t] = li++;
+            else pick[t] = ii++;
+        }
+        H.node[nxt] = H.node[pick[0]] + H.node[pick[1]];
+        H.parent[pick[0]] = H.parent[pick[1]] = static_cast<uint16_t>(nxt);
+        ++nxt;
+    }
+    H.depth[2u * n - 2u] = 0;
+    for (int k = static_cast<int>(2u * n) - 3; k >= 0; --k) H.depth[k] = static_cast<uint8_t>(H.depth[H.parent[k]] + 1u);
+    uint32_t bl[64];
+    for (uint32_t i = 0; i < 64; ++i) bl[i] = 0;
+    uint32_t maxlen = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        const uint32_t d = H.depth[k];
+        if (d >= 64u) return 0;
+        bl[d]++;
+        maxlen = max(maxlen, d);
+    }
+    for (uint32_t i = maxlen; i > kHufMaxBits; --i) {
+        while (bl[i] > 0) {
+            uint32_t j = i - 2u;
+            while (bl[j] == 0) --j;
+            bl[i] -= 2u;
+            bl[i - 1] += 1u;
+            bl[j + 1] += 2u;
+            bl[j] -= 1u;
+        }
+    }
+    for (uint32_t s2 = 0; s2 < 256; ++s2) H.len[s2] = 0;
+    uint32_t k = 0, maxb = 0;
+    for (uint32_t L = kHufMaxBits; L >= 1u; --L) {
+        for (uint32_t c = 0; c < bl[L]; ++c) H.len[H.leaf[k++]] = static_cast<uint8_t>(L);
+        if (bl[L] && !maxb) maxb = L;
+    }
+    uint32_t start[kHufMaxBits + 2];
+    start[maxb] = 0;
+    for (uint32_t L = maxb - 1; L >= 1u; --L) start[L] = (start[L + 1] + bl[L + 1]) >> 1;
+    uint32_t last = 0;
+    for (uint32_t s2 = 0; s2 < 256; ++s2) {
+        if (H.len[s2]) {
+            H.code[s2] = static_cast<uint16_t>(start[H.len[s2]]++);
+            last = s2;
+        }
+    }
+    const uint32_t N = last;  // the last byte's weight is implied
+    for (uint32_t s2 = 0; s2 < N; ++s2) H.wts[s2] = H.len[s2] ? static_cast<uint8_t>(maxb + 1u - H.len[s2]) : 0u;
+    if (N <= 128u) {
+        H.tree[0] = static_cast<uint8_t>(127u + N);
+        for (uint32_t i = 0; i < N; i += 2) {
+            const uint32_t hi4 = H.wts[i], lo4 = i + 1 < N ? H.wts[i + 1] : 0u;
+            H.tree[1 + i / 2] = static_cast<uint8_t>((hi4 << 4) | lo4);
+        }
+        H.tree_bytes = 1u + (N + 1u) / 2u;
+        return 1;
+    }
+    const uint32_t f = huf_fse_weights(H, N);
+    if (!f) return 0;
+    H.tree[0] = static_cast<uint8_t>(f);
+    H.tree_bytes = 1u + f;
+    return 1;
+}
+
+// Literal runs for the Huffman streams: with 4 streams, threads 64s .. 64s+63
+// split stream s; with one stream all threads split it.  Run j of a stream
+// covers [lo + j*size, lo + (j+1)*size); the stream's bits start with its last
+// literal, so the highest run comes first.
+struct LitRun {
+    uint32_t stream, j, group, lo, hi;
+};
+__device__ __forceinline__ LitRun lit_run(uint32_t tid, uint32_t nlit, uint32_t nstreams, uint32_t seg) {
+    LitRun r;
+    r.group = nstreams == 4u ? kLitThreads / 4u : kLitThreads;
+    r.stream = tid / r.group;
+    r.j = tid % r.group;
+    const uint32_t s_lo = r.stream * seg, s_hi = r.stream == nstreams - 1u ? nlit : s_lo + seg;
+    const uint32_t size = (s_hi - s_lo + r.group - 1u) / r.group;
+    r.lo = min(s_lo + r.j * size, s_hi);
+    r.hi = min(r.lo + size, s_hi);
+    return r;
+}
+
+// Writes the codes of lit[hi-1] .. lit[lo] (in that order) at bit `bitpos` of
+// the 32-bit-word array `out`; `marker` appends the end-of-stream bit.  Words
+// this run shares with a neighbour are ORed in atomically, the others stored.
+__device__ void huf_write_run(const HufSmem &H, const uint8_t *lit, uint32_t lo, uint32_t hi, uint32_t *out,
+                              uint64_t bitpos, bool marker) {
+    uint64_t word = bitpos >> 5;
+    uint32_t nb = static_cast<uint32_t>(bitpos & 31u);
+    uint64_t acc = 0;
+    bool first = true;
+    auto add = [&](uint32_t code, uint32_t len) {
+        acc |= static_cast<uint64_t>(code) << nb;
+        nb += len;
+        if (nb >= 32u) {
+            if (first) atomicOr(out + word, static_cast<uint32_t>(acc));
+            else out[word] = static_cast<uint32_t>(acc);
+            first = false;
+            ++word;
+            acc >>= 32;
+            nb -= 32u;
+        }
+    };
+    for (uint32_t k = hi; k > lo; --k) {
+        const uint32_t x = lit[k - 1];
+        add(H.code[x], H.len[x]);
+    }
+    if (marker) add(1u, 1u);
+    if (nb) atomicOr(out + word, static_cast<uint32_t>(acc));
+}
+
 __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) {
-    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow bytes
+    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow literal bytes, then HufSmem
+    HufSmem &H = *reinterpret_cast<HufSmem *>(lit + kMaxWindow);
     __shared__ uint32_t warp_ll[kLitThreads / 32], warp_pos[kLitThreads / 32];
     __shared__ uint32_t tot_ll, tot_pos, bad;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
@@ -240,8 +503,17 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
         const uint32_t ns = static_cast<uint32_t>(a.seq_offsets[b + 1] - s0);
         const uint4 *sq = a.seqs + s0;
         uint8_t *slot = a.slots + static_cast<uint64_t>(b) * kZencSlot;
+        const uint32_t fh = frame_header_bytes(w);
         if (tid == 0) bad = ns > kZencMaxSeqs ? 1u : 0u;
         __syncthreads();
+        if (ns == 0u) {  // no sequences: the raw block is smaller
+            if (tid == 0) {
+                write_frame_header(slot, w);
+                a.sec_off[b] = 0u;
+            }
+            __syncthreads();
+            continue;
+        }
         // Each thread owns a contiguous run of sequences; a block scan gives
         // its first literal's output index and source position.
         const uint32_t per = (ns + kLitThreads - 1) / kLitThreads;
@@ -266,6 +538,8 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             warp_ll[wid] = xll;
             warp_pos[wid] = xpos;
         }
+        if (tid < 256u) H.count[tid] = 0u;
+        if (tid < 4u) H.seg_bits[tid] = 0u;
         __syncthreads();
         uint32_t base_ll = 0, base_pos = 0;
         for (uint32_t k = 0; k < wid; ++k) {
@@ -298,27 +572,129 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
                 write_frame_header(slot, w);
                 a.sec_off[b] = 0;  // raw frame
             }
-        } else {
-            const uint32_t nlit = TLL + (w - TP);
-            const uint32_t fh = frame_header_bytes(w);
-            const uint32_t lh = nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
-            const uint32_t H = fh + 3u + lh;
-            for (uint32_t k = tid; k < nlit; k += kLitThreads) slot[H + k] = lit[k];
-            if (tid == 0) {
-                write_frame_header(slot, w);
-                uint8_t *h = slot + fh + 3u;
-                if (lh == 1u) {
-                    h[0] = static_cast<uint8_t>(nlit << 3);  // Raw_Literals_Block, Size_Format 00
-                } else if (lh == 2u) {
-                    h[0] = static_cast<uint8_t>(((nlit << 4) & 0xF0u) | (1u << 2));
+            __syncthreads();
+            continue;
+        }
+        const uint32_t nlit = TLL + (w - TP);
+        // histogram, then the present bytes ranked by (count, byte)
+        for (uint32_t k = tid; k < nlit; k += kLitThreads) atomicAdd(&H.count[lit[k]], 1u);
+        __syncthreads();
+        uint32_t c = 0;
+        if (tid < 256u) {
+            c = H.count[tid];
+            if (c) {
+                uint32_t r = 0;
+                for (uint32_t s2 = 0; s2 < 256; ++s2) {
+                    const uint32_t cs = H.count[s2];
+                    r += (cs != 0u && (cs < c || (cs == c && s2 < tid))) ? 1u : 0u;
+                }
+                H.leaf[r] = static_cast<uint16_t>(tid);
+            }
+        }
+        const uint32_t nsym = __syncthreads_count(c != 0u);
+        if (tid == 0) {
+            H.nsym = nsym;
+            H.huf_ok = nsym >= 2u ? huf_plan(H) : 0u;
+            H.seg = nlit < 1024u ? nlit : (nlit + 3u) / 4u;
+        }
+        __syncthreads();
+        const uint32_t nst_plan = nlit < 1024u ? 1u : 4u;
+        LitRun run{};
+        if (H.huf_ok) {  // exact bits of every run, and of every stream
+            run = lit_run(tid, nlit, nst_plan, H.seg);
+            uint32_t v = 0;
+            for (uint32_t k = run.lo; k < run.hi; ++k) v += H.len[lit[k]];
+            H.tbits[tid] = v;
+            uint32_t t = v;
+            for (uint32_t o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+            if (lane == 0 && t) atomicAdd(&H.seg_bits[run.stream], t);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            // choose the literal section and lay it out after the frame and block headers
+            const uint32_t L0 = fh + 3u;
+            const uint32_t raw_hdr = nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
+            uint32_t mode = 0, size = raw_hdr + nlit;  // 0 raw, 1 RLE, 2 Huffman
+            uint32_t hdr = 0, body = 0, nst = 0;
+            if (nsym == 1u) {
+                mode = 1;
+                size = raw_hdr + 1u;
+            } else if (H.huf_ok) {
+                nst = nlit < 1024u ? 1u : 4u;
+                uint32_t streams = 0;
+                for (uint32_t t = 0; t < nst; ++t) {
+                    H.stream_bytes[t] = (H.seg_bits[t] + 8u) >> 3;  // + end marker, rounded up
+                    streams += H.stream_bytes[t];
+                }
+                body = H.tree_bytes + (nst == 4u ? 6u : 0u) + streams;
+                hdr = nst == 1u ? 3u : (max(nlit, body) < 16384u ? 4u : 5u);
+                if ((nst == 1u && body >= 1024u) || hdr + body >= size) {
+                    nst = 0;
+                } else {
+                    mode = 2;
+                    size = hdr + body;
+                }
+            }
+            uint8_t *h = slot + L0;
+            write_frame_header(slot, w);
+            if (mode == 2) {
+                uint64_t v;
+                if (hdr == 3u) v = 2u | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 14);
+                else if (hdr == 4u) v = 2u | (2u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 18);
+                else v = 2u | (3u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 22);
+                for (uint32_t i = 0; i < hdr; ++i) h[i] = static_cast<uint8_t>(v >> (8u * i));
+                for (uint32_t i = 0; i < H.tree_bytes; ++i) h[hdr + i] = H.tree[i];
+                uint32_t o = L0 + hdr + H.tree_bytes;
+                if (nst == 4u) {
+                    for (uint32_t t = 0; t < 3; ++t) {
+                        slot[o + 2 * t] = static_cast<uint8_t>(H.stream_bytes[t]);
+                        slot[o + 2 * t + 1] = static_cast<uint8_t>(H.stream_bytes[t] >> 8);
+                    }
+                    o += 6u;
+                }
+                for (uint32_t t = 0; t < nst; ++t) {
+                    H.stream_off[t] = o;
+                    o += H.stream_bytes[t];
+                }
+            } else {
+                const uint32_t type = mode;  // Raw_Literals_Block 0, RLE_Literals_Block 1
+                if (raw_hdr == 1u) {
+                    h[0] = static_cast<uint8_t>(type | (nlit << 3));
+                } else if (raw_hdr == 2u) {
+                    h[0] = static_cast<uint8_t>(type | (1u << 2) | ((nlit << 4) & 0xF0u));
                     h[1] = static_cast<uint8_t>(nlit >> 4);
                 } else {
-                    h[0] = static_cast<uint8_t>(((nlit << 4) & 0xF0u) | (3u << 2));
+                    h[0] = static_cast<uint8_t>(type | (3u << 2) | ((nlit << 4) & 0xF0u));
                     h[1] = static_cast<uint8_t>(nlit >> 4);
                     h[2] = static_cast<uint8_t>(nlit >> 12);
                 }
-                a.sec_off[b] = ns ? H + nlit : 0u;  // no sequences: the raw block is smaller
+                if (mode == 1u) h[raw_hdr] = lit[0];
             }
+            H.mode = mode;
+            H.nstreams = nst;
+            a.sec_off[b] = L0 + size;
+        }
+        __syncthreads();
+        if (H.mode == 0u) {
+            const uint32_t raw_hdr = nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
+            uint8_t *dst = slot + fh + 3u + raw_hdr;
+            for (uint32_t k = tid; k < nlit; k += kLitThreads) dst[k] = lit[k];
+        } else if (H.mode == 2u) {
+            // The streams' bytes start at zero (runs OR their shared words in); the
+            // words that hold the last header bytes are kept.
+            const uint32_t s0b = H.stream_off[0];
+            const uint32_t s1b = H.stream_off[H.nstreams - 1u] + H.stream_bytes[H.nstreams - 1u];
+            uint32_t *wslot = reinterpret_cast<uint32_t *>(slot);
+            const uint32_t w0 = (s0b + 3u) >> 2, w1 = (s1b + 3u) >> 2;
+            for (uint32_t k = s0b + tid; k < min(w0 * 4u, s1b); k += kLitThreads) slot[k] = 0;
+            for (uint32_t k = w0 + tid; k < w1; k += kLitThreads) wslot[k] = 0u;
+            __syncthreads();
+            // bit offset of this run: the runs after it in the stream come first
+            uint32_t off = 0;
+            for (uint32_t j2 = run.j + 1u; j2 < run.group; ++j2) off += H.tbits[run.stream * run.group + j2];
+            const uint64_t bitpos = 8ull * H.stream_off[run.stream] + off;
+            if (run.hi > run.lo || run.j == 0u)
+                huf_write_run(H, lit, run.lo, run.hi, wslot, bitpos, run.j == 0u);
         }
         __syncthreads();
     }
@@ -604,11 +980,11 @@ unsigned long long g_lit_smem_set = 0, g_seq_smem_set = 0;
 cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st) {
     if (l.num_windows == 0) return cudaSuccess;
     const ZencArgs a = args_of(l);
-    cudaError_t e = set_smem_once(zenc_literals_kernel, kMaxWindow, g_lit_smem_set);
+    cudaError_t e = set_smem_once(zenc_literals_kernel, kLitSmem, g_lit_smem_set);
     if (e != cudaSuccess) return e;
     int grid = l.num_sms * 3;
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    zenc_literals_kernel<<<grid, kLitThreads, kMaxWindow, st>>>(a);
+    zenc_literals_kernel<<<grid, kLitThreads, kLitSmem, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = set_smem_once(zenc_sequences_kernel, sizeof(SeqSmem), g_seq_smem_set)) != cudaSuccess) return e;
     grid = l.num_sms * 3;

@@ -18,14 +18,28 @@ INPUTS = [
     {"kind": "text", "n": 70000, "seed": 42},
     {"kind": "zeros", "n": 100000},
     {"kind": "random", "n": 70000, "seed": 3},
+    {"kind": "zipf", "n": 2 * W + 300, "seed": 4},   # all 256 byte values: FSE-coded Huffman weights
+    {"kind": "fib", "n": W + 5000, "seed": 5},       # Fibonacci counts: code lengths limited to 11
+    {"kind": "zipf", "n": 900, "seed": 6},           # one Huffman stream
 ]
 
 
 def _build(spec):
+    rng = np.random.default_rng(spec.get("seed", 0))
+    n = spec["n"]
     if spec["kind"] == "zeros":
-        return np.zeros(spec["n"], np.uint8)
+        return np.zeros(n, np.uint8)
     if spec["kind"] == "random":
-        return np.frombuffer(np.random.default_rng(spec["seed"]).bytes(spec["n"]), np.uint8).copy()
+        return np.frombuffer(rng.bytes(n), np.uint8).copy()
+    if spec["kind"] == "zipf":
+        p = 1.0 / np.arange(1, 257) ** 1.1
+        return rng.permutation(256)[rng.choice(256, n, p=p / p.sum())].astype(np.uint8)
+    if spec["kind"] == "fib":
+        f = [1, 1]
+        while len(f) < 24:
+            f.append(f[-1] + f[-2])
+        p = np.array(f, float)
+        return (rng.choice(24, n, p=p / p.sum()) + 150).astype(np.uint8)
     return cases.build(spec)
 
 

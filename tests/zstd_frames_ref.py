@@ -1,8 +1,9 @@
 """Pure-Python restatement of the GPU Zstd entropy stage (test checker only):
 one frame per window from its ZSTD_Sequence records, following RFC 8878 --
-single-segment frame header, one block, Raw_Literals_Block, sequences in
-Predefined_Mode with repeat-offset codes -- or a raw block when the compressed
-block would not be smaller than the window.  The tests compare the GPU frames
+single-segment frame header, one block, literals raw, RLE or Huffman-coded
+(whichever is smallest), sequences in Predefined_Mode with repeat-offset codes
+-- or a raw block when the compressed block would not be smaller than the
+window.  The tests compare the GPU frames
 with these byte for byte and decode both with stock libzstd."""
 
 LL_NORM = [4, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2, 2, 2, 3, 2, 1, 1, 1, 1, 1,
@@ -80,6 +81,233 @@ def _block_header(btype, size):
     return (1 | (btype << 1) | (size << 3)).to_bytes(3, "little")
 
 
+# ------------------------------------------------------------------ literals
+
+HUF_MAX_BITS = 11
+
+
+def _huffman_lengths(counts):
+    """Code lengths of a Huffman code over the present symbols (two queues;
+    leaves sorted by (count, symbol); on equal counts the leaf is taken
+    first), limited to HUF_MAX_BITS by moving pairs of leaves up the tree
+    while keeping the code complete."""
+    leaves = sorted((c, s) for s, c in enumerate(counts) if c)
+    n = len(leaves)
+    cnt = [c for c, _ in leaves] + [0] * (n - 1)
+    parent = [0] * (2 * n - 1)
+    li, ii, nxt = 0, n, n
+
+    def pop():
+        nonlocal li, ii
+        if li < n and (ii >= nxt or cnt[li] <= cnt[ii]):
+            li += 1
+            return li - 1
+        ii += 1
+        return ii - 1
+
+    while nxt < 2 * n - 1:
+        a = pop()
+        b = pop()
+        cnt[nxt] = cnt[a] + cnt[b]
+        parent[a] = parent[b] = nxt
+        nxt += 1
+    depth = [0] * (2 * n - 1)
+    for k in range(2 * n - 3, -1, -1):
+        depth[k] = depth[parent[k]] + 1
+    bl = [0] * 64
+    for k in range(n):
+        bl[depth[k]] += 1
+    maxlen = max(depth[:n])
+    for i in range(maxlen, HUF_MAX_BITS, -1):
+        while bl[i] > 0:
+            j = i - 2
+            while bl[j] == 0:
+                j -= 1
+            bl[i] -= 2
+            bl[i - 1] += 1
+            bl[j + 1] += 2
+            bl[j] -= 1
+    # longest codes to the least frequent symbols
+    lens = [0] * 256
+    k = 0
+    for length in range(HUF_MAX_BITS, 0, -1):
+        for _ in range(bl[length]):
+            lens[leaves[k][1]] = length
+            k += 1
+    return lens
+
+
+def _canonical_codes(lens):
+    maxb = max(lens)
+    bl = [0] * (maxb + 2)
+    for l in lens:
+        if l:
+            bl[l] += 1
+    start = [0] * (maxb + 2)
+    for l in range(maxb - 1, 0, -1):
+        start[l] = (start[l + 1] + bl[l + 1]) >> 1
+    codes = [0] * 256
+    for s in range(256):
+        if lens[s]:
+            codes[s] = start[lens[s]]
+            start[lens[s]] += 1
+    return codes
+
+
+def _ncount_bits(norm, al, bits):
+    """FSE table description (RFC 8878 4.1.1) of `norm` (no -1 entries)."""
+    bits.add(al - 5, 4)
+    remaining, threshold, nb = (1 << al) + 1, 1 << al, al + 1
+    last = max(s for s, c in enumerate(norm) if c)
+    s = 0
+    while s <= last:
+        v = norm[s] + 1
+        mx = (2 * threshold - 1) - remaining
+        if v < mx:
+            bits.add(v, nb - 1)
+        elif v < threshold:
+            bits.add(v, nb)
+        else:
+            bits.add(v + mx, nb)
+        remaining -= norm[s]
+        while remaining < threshold:
+            nb -= 1
+            threshold >>= 1
+        if norm[s] == 0:
+            z = 0
+            while s + 1 + z < last and norm[s + 1 + z] == 0:
+                z += 1
+            s += z
+            while z >= 3:
+                bits.add(3, 2)
+                z -= 3
+            bits.add(z, 2)
+        s += 1
+
+
+def _fse_dec_table(norm, al):
+    size = 1 << al
+    mask, step, high = size - 1, (size >> 1) + (size >> 3) + 3, size - 1
+    sym = [0] * size
+    nxt = list(norm)
+    pos = 0
+    for s, c in enumerate(norm):
+        for _ in range(c):
+            sym[pos] = s
+            pos = (pos + step) & mask
+            while pos > high:
+                pos = (pos + step) & mask
+    nbits, base = [0] * size, [0] * size
+    for u in range(size):
+        x = nxt[sym[u]]
+        nxt[sym[u]] += 1
+        nbits[u] = al - (x.bit_length() - 1)
+        base[u] = (x << nbits[u]) - size
+    return sym, nbits, base
+
+
+def _fse_weights(weights):
+    """FSE-compressed Huffman weights (accuracy 6, two interleaved states), or
+    None when that is not possible or larger than 127 bytes."""
+    al, size = 6, 64
+    n = len(weights)
+    cw = [0] * 12
+    for w in weights:
+        cw[w] += 1
+    if sum(1 for c in cw if c) < 2:
+        return None
+    norm = [0 if c == 0 else max(1, c * size // n) for c in cw]
+    big = max(range(12), key=lambda s: (norm[s], -s))
+    norm[big] += size - sum(norm)
+    if norm[big] <= 0:
+        return None
+    sym, nbits, base = _fse_dec_table(norm, al)
+    enc = {}
+    for u in range(size):
+        for v in range(base[u], base[u] + (1 << nbits[u])):
+            enc[(sym[u], v)] = u
+    bits = _Bits()
+    _ncount_bits(norm, al, bits)
+    desc = bits.v.to_bytes((bits.n + 7) // 8, "little")
+    st = [0] * n
+    st[n - 1] = next(u for u in range(size) if sym[u] == weights[n - 1])
+    st[n - 2] = next(u for u in range(size) if sym[u] == weights[n - 2] and nbits[u] >= 1)
+    for i in range(n - 3, -1, -1):
+        st[i] = enc[(weights[i], st[i + 2])]
+    b2 = _Bits()
+    for i in range(n - 3, -1, -1):
+        b2.add(st[i + 2] - base[st[i]], nbits[st[i]])
+    b2.add(st[1], al)
+    b2.add(st[0], al)
+    out = desc + b2.close()
+    return out if len(out) <= 127 else None
+
+
+def _huf_stream(data, lens, codes):
+    bits = _Bits()
+    for x in reversed(data):
+        bits.add(codes[x], lens[x])
+    return bits.close()
+
+
+def _raw_lit_header(btype, n):
+    if n < 32:
+        return bytes([btype | (n << 3)])
+    if n < 4096:
+        return bytes([btype | 4 | ((n << 4) & 0xF0), n >> 4])
+    return bytes([btype | 12 | ((n << 4) & 0xF0), (n >> 4) & 0xFF, n >> 12])
+
+
+def literals_section(lits):
+    """Smallest of: raw, RLE (one distinct byte), Huffman-compressed (1 stream
+    below 1024 literals, else 4 streams)."""
+    lits = bytes(lits)
+    nl = len(lits)
+    raw = _raw_lit_header(0, nl) + lits
+    if nl == 0:
+        return raw
+    counts = [0] * 256
+    for x in lits:
+        counts[x] += 1
+    if sum(1 for c in counts if c) == 1:
+        return _raw_lit_header(1, nl) + lits[:1]
+    lens = _huffman_lengths(counts)
+    maxb = max(lens)
+    last = max(s for s in range(256) if counts[s])
+    weights = [(maxb + 1 - lens[s]) if lens[s] else 0 for s in range(last)]
+    if len(weights) <= 128:
+        packed = bytes([127 + len(weights)])
+        ws = weights + [0]
+        packed += bytes((ws[i] << 4) | ws[i + 1] for i in range(0, len(weights), 2))
+        tree = packed
+    else:
+        f = _fse_weights(weights)
+        if f is None:
+            return raw
+        tree = bytes([len(f)]) + f
+    codes = _canonical_codes(lens)
+    if nl < 1024:
+        streams = [_huf_stream(lits, lens, codes)]
+        body = tree + streams[0]
+        if len(body) >= 1024:
+            return raw
+        hdr = (2 | (0 << 2) | (nl << 4) | (len(body) << 14)).to_bytes(3, "little")
+    else:
+        seg = (nl + 3) // 4
+        parts = [lits[k * seg:(k + 1) * seg] for k in range(3)] + [lits[3 * seg:]]
+        streams = [_huf_stream(p, lens, codes) for p in parts]
+        if any(len(s) > 65535 for s in streams[:3]):
+            return raw
+        body = tree + b"".join(len(s).to_bytes(2, "little") for s in streams[:3]) + b"".join(streams)
+        m = max(nl, len(body))
+        if m < 16384:
+            hdr = (2 | (2 << 2) | (nl << 4) | (len(body) << 18)).to_bytes(4, "little")
+        else:
+            hdr = (2 | (3 << 2) | (nl << 4) | (len(body) << 22)).to_bytes(5, "little")
+    out = hdr + body
+    return out if len(out) < len(raw) else raw
+
+
 def encode_frame(win, seqs):
     """win: bytes of one window; seqs: iterable of (offset, litLength, matchLength)."""
     win = bytes(win)
@@ -94,13 +322,7 @@ def encode_frame(win, seqs):
         lits += win[pos:pos + ll]
         pos += ll + ml
     lits += win[pos:]
-    nl = len(lits)
-    if nl < 32:
-        lh = bytes([nl << 3])
-    elif nl < 4096:
-        lh = bytes([((nl << 4) & 0xF0) | 4, nl >> 4])
-    else:
-        lh = bytes([((nl << 4) & 0xF0) | 12, (nl >> 4) & 0xFF, nl >> 12])
+    lsec = literals_section(lits)
     ns = len(seqs)
     sh = bytes([ns]) if ns < 128 else bytes([(ns >> 8) + 0x80, ns & 0xFF])
     sh += b"\x00"
@@ -146,7 +368,7 @@ def encode_frame(win, seqs):
     bits.add(dml, ML_LOG)
     bits.add(dof, OF_LOG)
     bits.add(dll, LL_LOG)
-    content = lh + bytes(lits) + sh + bits.close()
+    content = lsec + sh + bits.close()
     if len(content) >= w:
         return raw
     return fh + _block_header(2, len(content)) + content
