@@ -37,7 +37,7 @@ struct EventPair {
 // Device scratch of one match-find step.
 struct Scratch {
     DevBuf packed, counts, cand, seg;
-    DevBuf zslots, zovs, zaux;  // Zstd entropy stage: frame slots, offset codes, per-window words
+    DevBuf zslots, zovs, zaux, zplan;  // Zstd entropy stage: frame slots, offset codes, per-window words, plans
 };
 
 // One stage of the host-buffer pipeline: its own stream, input, scratch and
@@ -277,6 +277,7 @@ int zenc_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, const voi
     if ((r = ensure_dev(c, sc.zslots, nb * (size_t)gcz::kZencSlot)) != GCZ_OK) return r;
     if ((r = ensure_dev(c, sc.zovs, nb * (size_t)gcz::kZencMaxSeqs * 4)) != GCZ_OK) return r;
     if ((r = ensure_dev(c, sc.zaux, nb * 12 + 64)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sc.zplan, nb * ((size_t)gcz::kZencPlanBytes + 1024))) != GCZ_OK) return r;
     gcz::ZencLaunch l{};
     l.src = d_src;
     l.n = n;
@@ -289,12 +290,14 @@ int zenc_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, const voi
     l.sec_off = static_cast<uint32_t *>(sc.zaux.p);
     l.fsize = l.sec_off + nb;
     l.raw = reinterpret_cast<uint8_t *>(l.fsize + nb);
+    l.plan = static_cast<uint8_t *>(sc.zplan.p);
+    l.hist = reinterpret_cast<uint32_t *>(l.plan + nb * (size_t)gcz::kZencPlanBytes);
     l.status = c->d_status;
     l.num_sms = c->num_sms;
     GCZ_CUDA(c, gcz::launch_zenc(l, st));
     GCZ_CUDA(c, gcz::launch_scan_counts(l.fsize, (uint32_t)nb, d_frame_offsets, st));
     GCZ_CUDA(c, gcz::launch_zenc_compact(l, d_frame_offsets, d_out, out_capacity, st));
-    c->all_launches += 4;
+    c->all_launches += 6;
     return GCZ_OK;
 }
 
@@ -362,7 +365,7 @@ extern "C" void gcz_destroy(gcz_ctx *c) {
         DeviceGuard g(c->device);
         cudaStreamSynchronize(c->stream);
         auto free_scratch = [](Scratch &x) {
-            for (DevBuf *b : {&x.packed, &x.counts, &x.cand, &x.seg, &x.zslots, &x.zovs, &x.zaux})
+            for (DevBuf *b : {&x.packed, &x.counts, &x.cand, &x.seg, &x.zslots, &x.zovs, &x.zaux, &x.zplan})
                 if (b->p) cudaFree(b->p);
         };
         free_scratch(c->sc);

@@ -84,6 +84,7 @@ cudaError_t launch_zstd_literals(const uint8_t *src, uint64_t n, uint32_t window
 // Zstd entropy stage (gcz_zenc.cu): frames from ZSTD_Sequence records.
 constexpr uint32_t kZencSlot = 65536 + 1024;  // per-window frame slot bytes
 constexpr uint32_t kZencMaxSeqs = 21845;      // sequences per window (chunk_size / 3)
+constexpr uint32_t kZencPlanBytes = 1024;     // per-window Huffman plan record
 struct ZencLaunch {
     const uint8_t *src;           // windows at b * window
     uint64_t n;
@@ -96,6 +97,8 @@ struct ZencLaunch {
     uint32_t *sec_off;            // num_windows
     uint32_t *fsize;              // num_windows
     uint8_t *raw;                 // num_windows
+    uint32_t *hist;               // num_windows * 256
+    uint8_t *plan;                // num_windows * kZencPlanBytes
     uint32_t *status;
     int num_sms;
 };

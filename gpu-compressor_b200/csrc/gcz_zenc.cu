@@ -198,6 +198,8 @@ struct ZencArgs {
     uint32_t *sec_off;         // start of the sequences section in the slot (0 = raw frame)
     uint32_t *fsize;           // frame bytes
     uint8_t *raw;              // 1 = raw block
+    uint32_t *hist;            // 256 literal-byte counts per window
+    uint8_t *plan;             // kZencPlanBytes per window
     uint32_t *status;
 };
 
@@ -242,258 +244,51 @@ __device__ __forceinline__ void write_block_header(uint8_t *p, uint32_t type, ui
 // largest absorbing the remainder; two interleaved states; the state of the
 // second-to-last weight is chosen with at least one update bit, so that the
 // decoder's last update runs past the stream start and decoding ends there.
+//
+// Three kernels: zenc_literals_kernel gathers each window's literals, writes
+// the raw literal section (the default) and the byte histogram;
+// zenc_huf_plan_kernel builds the code of a window in one warp (many windows
+// per SM, so the serial steps of one overlap the others');
+// zenc_huf_write_kernel rewrites the section as RLE or Huffman-coded where
+// that is smaller.
 constexpr uint32_t kHufMaxBits = 11;
 
-struct HufSmem {
-    uint32_t count[256];
-    uint32_t node[511];   // node weights, leaves first
-    uint16_t leaf[256];   // present bytes by ascending (count, byte)
-    uint16_t parent[511];
-    uint8_t depth[511];
+// Per-window record from the plan to the write kernel.
+struct PlanRec {
     uint8_t len[256];
     uint16_t code[256];
-    uint8_t tree[132];    // Huffman_Tree_Description
-    uint8_t wts[256];     // transmitted weights
-    uint8_t st[256];      // FSE states of the weights
-    uint8_t fsym[64], fnb[64], fbase[64];
-    uint8_t fenc[12 * 64];
-    uint32_t seg_bits[4];
-    uint32_t tbits[kLitThreads];  // bits of each thread's run of literals
-    uint32_t nsym, tree_bytes, huf_ok, mode, nstreams, seg;
-    uint32_t stream_off[4], stream_bytes[4];
+    uint8_t tree[132];  // Huffman_Tree_Description
+    uint32_t tree_bytes;
+    uint32_t mode;  // 0: keep raw, 1: RLE, 2: Huffman candidate
+    uint32_t nlit;
+    uint32_t rle;
 };
-constexpr uint32_t kLitSmem = kMaxWindow + sizeof(HufSmem);
+static_assert(sizeof(PlanRec) <= kZencPlanBytes, "plan record");
 
-// Bits into a byte buffer in shared memory, LSB first.
-struct SmemBits {
-    uint8_t *p;
-    uint32_t cap, pos, nbits;
-    uint64_t acc;
-    bool ovf;
-    __device__ void add(uint32_t v, uint32_t nb) {
-        acc |= static_cast<uint64_t>(v) << nbits;
-        nbits += nb;
-        while (nbits >= 8u) {
-            if (pos < cap) p[pos] = static_cast<uint8_t>(acc);
-            else ovf = true;
-            ++pos;
-            acc >>= 8;
-            nbits -= 8u;
-        }
+__device__ __forceinline__ uint32_t raw_lit_header_bytes(uint32_t nlit) {
+    return nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
+}
+__device__ void write_raw_lit_header(uint8_t *h, uint32_t type, uint32_t nlit) {
+    const uint32_t hb = raw_lit_header_bytes(nlit);
+    if (hb == 1u) {
+        h[0] = static_cast<uint8_t>(type | (nlit << 3));
+    } else if (hb == 2u) {
+        h[0] = static_cast<uint8_t>(type | (1u << 2) | ((nlit << 4) & 0xF0u));
+        h[1] = static_cast<uint8_t>(nlit >> 4);
+    } else {
+        h[0] = static_cast<uint8_t>(type | (3u << 2) | ((nlit << 4) & 0xF0u));
+        h[1] = static_cast<uint8_t>(nlit >> 4);
+        h[2] = static_cast<uint8_t>(nlit >> 12);
     }
-    __device__ void flush() {  // pad the last partial byte with zeros
-        if (nbits) add(0u, 8u - nbits);
-    }
-    __device__ void close() {  // end marker, then pad
-        add(1u, 1u);
-        flush();
-    }
-};
-
-// FSE-compressed weights H.wts[0..N) into H.tree + 1; returns its size, or 0.
-__device__ uint32_t huf_fse_weights(HufSmem &H, uint32_t N) {
-    uint32_t cw[12] = {0};
-    for (uint32_t i = 0; i < N; ++i) cw[H.wts[i]]++;
-    uint32_t distinct = 0;
-    for (uint32_t s2 = 0; s2 < 12; ++s2) distinct += cw[s2] ? 1u : 0u;
-    if (distinct < 2) return 0;
-    int norm[12];
-    int sum = 0, big = 0;
-    for (uint32_t s2 = 0; s2 < 12; ++s2) {
-        norm[s2] = cw[s2] ? max(1, static_cast<int>(cw[s2] * 64u / N)) : 0;
-        sum += norm[s2];
-        if (norm[s2] > norm[big]) big = static_cast<int>(s2);
-    }
-    norm[big] += 64 - sum;
-    if (norm[big] <= 0) return 0;
-    // decoder table (no "less than 1" entries, so no high threshold) and encoder map
-    uint32_t pos = 0;
-    for (uint32_t s2 = 0; s2 < 12; ++s2)
-        for (int c = 0; c < norm[s2]; ++c) {
-            H.fsym[pos] = static_cast<uint8_t>(s2);
-            pos = (pos + 43u) & 63u;  // step (64 >> 1) + (64 >> 3) + 3
-        }
-    uint32_t nxt[12];
-    for (uint32_t s2 = 0; s2 < 12; ++s2) nxt[s2] = static_cast<uint32_t>(norm[s2]);
-    for (uint32_t u = 0; u < 64; ++u) {
-        const uint32_t x = nxt[H.fsym[u]]++;
-        const uint32_t nb = 6u - highbit(x);
-        H.fnb[u] = static_cast<uint8_t>(nb);
-        H.fbase[u] = static_cast<uint8_t>((x << nb) - 64u);
-        for (uint32_t v = H.fbase[u]; v < H.fbase[u] + (1u << nb); ++v) H.fenc[H.fsym[u] * 64u + v] = static_cast<uint8_t>(u);
-    }
-    // table description (RFC 8878 4.1.1)
-    SmemBits wr{H.tree + 1, 127u, 0u, 0u, 0ull, false};
-    wr.add(1u, 4u);  // accuracy 6
-    int remaining = 65, threshold = 64;
-    uint32_t nb = 7;
-    int lastw = 11;
-    while (norm[lastw] == 0) --lastw;
-    for (int s2 = 0; s2 <= lastw; ++s2) {
-        const int v = norm[s2] + 1, mx = (2 * threshold - 1) - remaining;
-        if (v < mx) wr.add(static_cast<uint32_t>(v), nb - 1u);
-        else if (v < threshold) wr.add(static_cast<uint32_t>(v), nb);
-        else wr.add(static_cast<uint32_t>(v + mx), nb);
-        remaining -= norm[s2];
-        while (remaining < threshold) {
-            --nb;
-            threshold >>= 1;
-        }
-        if (norm[s2] == 0) {
-            int z = 0;
-            while (s2 + 1 + z < lastw && norm[s2 + 1 + z] == 0) ++z;
-            s2 += z;
-            for (; z >= 3; z -= 3) wr.add(3u, 2u);
-            wr.add(static_cast<uint32_t>(z), 2u);
-        }
-    }
-    wr.flush();
-    // states: the last two weights pick their states, the rest follow the chain
-    const uint32_t w1 = H.wts[N - 1], w2 = H.wts[N - 2];
-    uint32_t s_last = 64, s_prev = 64;
-    for (uint32_t u = 0; u < 64; ++u) {
-        if (s_last == 64 && H.fsym[u] == w1) s_last = u;
-        if (s_prev == 64 && H.fsym[u] == w2 && H.fnb[u] >= 1u) s_prev = u;
-    }
-    if (s_prev == 64) return 0;
-    H.st[N - 1] = static_cast<uint8_t>(s_last);
-    H.st[N - 2] = static_cast<uint8_t>(s_prev);
-    for (int i = static_cast<int>(N) - 3; i >= 0; --i) H.st[i] = H.fenc[H.wts[i] * 64u + H.st[i + 2]];
-    SmemBits bs{H.tree + 1 + wr.pos, 127u > wr.pos ? 127u - wr.pos : 0u, 0u, 0u, 0ull, false};
-    for (int i = static_cast<int>(N) - 3; i >= 0; --i) {
-        const uint32_t sti = H.st[i];
-        bs.add(H.st[i + 2] - H.fbase[sti], H.fnb[sti]);
-    }
-    bs.add(H.st[1], 6u);
-    bs.add(H.st[0], 6u);
-    bs.close();
-    if (wr.ovf || bs.ovf || wr.pos + bs.pos > 127u) return 0;
-    return wr.pos + bs.pos;
 }
 
-// Thread 0: code lengths, canonical codes and the tree description from
-// H.count / H.leaf (H.nsym >= 2 present bytes).  Returns 1 when usable.
-__device__ uint32_t huf_plan(HufSmem &H) {
-    const uint32_t n = H.nsym;
-    for (uint32_t k = 0; k < n; ++k) H.node[k] = H.count[H.leaf[k]];
-    uint32_t li = 0, ii = n, nxt = n;
-    while (nxt < 2u * n - 1u) {
-        uint32_t pick[2];
-        for (uint32_t t = 0; t < 2; ++t) {
-            if (li < n && (ii >= nxt || H.node[li] <= H.node[ii])) pick[t] = li++;
-            else pick[t] = ii++;
-        }
-        H.node[nxt] = H.node[pick[0]] + H.node[pick[1]];
-        H.parent[pick[0]] = H.parent[pick[1]] = static_cast<uint16_t>(nxt);
-        ++nxt;
-    }
-    H.depth[2u * n - 2u] = 0;
-    for (int k = static_cast<int>(2u * n) - 3; k >= 0; --k) H.depth[k] = static_cast<uint8_t>(H.depth[H.parent[k]] + 1u);
-    uint32_t bl[64];
-    for (uint32_t i = 0; i < 64; ++i) bl[i] = 0;
-    uint32_t maxlen = 0;
-    for (uint32_t k = 0; k < n; ++k) {
-        const uint32_t d = H.depth[k];
-        if (d >= 64u) return 0;
-        bl[d]++;
-        maxlen = max(maxlen, d);
-    }
-    for (uint32_t i = maxlen; i > kHufMaxBits; --i) {
-        while (bl[i] > 0) {
-            uint32_t j = i - 2u;
-            while (bl[j] == 0) --j;
-            bl[i] -= 2u;
-            bl[i - 1] += 1u;
-            bl[j + 1] += 2u;
-            bl[j] -= 1u;
-        }
-    }
-    for (uint32_t s2 = 0; s2 < 256; ++s2) H.len[s2] = 0;
-    uint32_t k = 0, maxb = 0;
-    for (uint32_t L = kHufMaxBits; L >= 1u; --L) {
-        for (uint32_t c = 0; c < bl[L]; ++c) H.len[H.leaf[k++]] = static_cast<uint8_t>(L);
-        if (bl[L] && !maxb) maxb = L;
-    }
-    uint32_t start[kHufMaxBits + 2];
-    start[maxb] = 0;
-    for (uint32_t L = maxb - 1; L >= 1u; --L) start[L] = (start[L + 1] + bl[L + 1]) >> 1;
-    uint32_t last = 0;
-    for (uint32_t s2 = 0; s2 < 256; ++s2) {
-        if (H.len[s2]) {
-            H.code[s2] = static_cast<uint16_t>(start[H.len[s2]]++);
-            last = s2;
-        }
-    }
-    const uint32_t N = last;  // the last byte's weight is implied
-    for (uint32_t s2 = 0; s2 < N; ++s2) H.wts[s2] = H.len[s2] ? static_cast<uint8_t>(maxb + 1u - H.len[s2]) : 0u;
-    if (N <= 128u) {
-        H.tree[0] = static_cast<uint8_t>(127u + N);
-        for (uint32_t i = 0; i < N; i += 2) {
-            const uint32_t hi4 = H.wts[i], lo4 = i + 1 < N ? H.wts[i + 1] : 0u;
-            H.tree[1 + i / 2] = static_cast<uint8_t>((hi4 << 4) | lo4);
-        }
-        H.tree_bytes = 1u + (N + 1u) / 2u;
-        return 1;
-    }
-    const uint32_t f = huf_fse_weights(H, N);
-    if (!f) return 0;
-    H.tree[0] = static_cast<uint8_t>(f);
-    H.tree_bytes = 1u + f;
-    return 1;
-}
-
-// Literal runs for the Huffman streams: with 4 streams, threads 64s .. 64s+63
-// split stream s; with one stream all threads split it.  Run j of a stream
-// covers [lo + j*size, lo + (j+1)*size); the stream's bits start with its last
-// literal, so the highest run comes first.
-struct LitRun {
-    uint32_t stream, j, group, lo, hi;
-};
-__device__ __forceinline__ LitRun lit_run(uint32_t tid, uint32_t nlit, uint32_t nstreams, uint32_t seg) {
-    LitRun r;
-    r.group = nstreams == 4u ? kLitThreads / 4u : kLitThreads;
-    r.stream = tid / r.group;
-    r.j = tid % r.group;
-    const uint32_t s_lo = r.stream * seg, s_hi = r.stream == nstreams - 1u ? nlit : s_lo + seg;
-    const uint32_t size = (s_hi - s_lo + r.group - 1u) / r.group;
-    r.lo = min(s_lo + r.j * size, s_hi);
-    r.hi = min(r.lo + size, s_hi);
-    return r;
-}
-
-// Writes the codes of lit[hi-1] .. lit[lo] (in that order) at bit `bitpos` of
-// the 32-bit-word array `out`; `marker` appends the end-of-stream bit.  Words
-// this run shares with a neighbour are ORed in atomically, the others stored.
-__device__ void huf_write_run(const HufSmem &H, const uint8_t *lit, uint32_t lo, uint32_t hi, uint32_t *out,
-                              uint64_t bitpos, bool marker) {
-    uint64_t word = bitpos >> 5;
-    uint32_t nb = static_cast<uint32_t>(bitpos & 31u);
-    uint64_t acc = 0;
-    bool first = true;
-    auto add = [&](uint32_t code, uint32_t len) {
-        acc |= static_cast<uint64_t>(code) << nb;
-        nb += len;
-        if (nb >= 32u) {
-            if (first) atomicOr(out + word, static_cast<uint32_t>(acc));
-            else out[word] = static_cast<uint32_t>(acc);
-            first = false;
-            ++word;
-            acc >>= 32;
-            nb -= 32u;
-        }
-    };
-    for (uint32_t k = hi; k > lo; --k) {
-        const uint32_t x = lit[k - 1];
-        add(H.code[x], H.len[x]);
-    }
-    if (marker) add(1u, 1u);
-    if (nb) atomicOr(out + word, static_cast<uint32_t>(acc));
-}
-
+// Gathers the literals of each window into shared memory (one CTA per
+// window), validates the sequences, writes frame header + raw literal
+// section into the slot and the histogram of the literal bytes.
 __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) {
-    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow literal bytes, then HufSmem
-    HufSmem &H = *reinterpret_cast<HufSmem *>(lit + kMaxWindow);
+    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow literal bytes
     __shared__ uint32_t warp_ll[kLitThreads / 32], warp_pos[kLitThreads / 32];
+    __shared__ uint32_t hist[256];
     __shared__ uint32_t tot_ll, tot_pos, bad;
     const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
     for (uint32_t b = blockIdx.x; b < a.num_windows; b += gridDim.x) {
@@ -503,13 +298,16 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
         const uint32_t ns = static_cast<uint32_t>(a.seq_offsets[b + 1] - s0);
         const uint4 *sq = a.seqs + s0;
         uint8_t *slot = a.slots + static_cast<uint64_t>(b) * kZencSlot;
+        PlanRec *plan = reinterpret_cast<PlanRec *>(a.plan + static_cast<uint64_t>(b) * kZencPlanBytes);
         const uint32_t fh = frame_header_bytes(w);
         if (tid == 0) bad = ns > kZencMaxSeqs ? 1u : 0u;
+        hist[tid] = 0u;  // kLitThreads == 256
         __syncthreads();
         if (ns == 0u) {  // no sequences: the raw block is smaller
             if (tid == 0) {
                 write_frame_header(slot, w);
                 a.sec_off[b] = 0u;
+                plan->nlit = 0u;
             }
             __syncthreads();
             continue;
@@ -538,8 +336,6 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             warp_ll[wid] = xll;
             warp_pos[wid] = xpos;
         }
-        if (tid < 256u) H.count[tid] = 0u;
-        if (tid < 4u) H.seg_bits[tid] = 0u;
         __syncthreads();
         uint32_t base_ll = 0, base_pos = 0;
         for (uint32_t k = 0; k < wid; ++k) {
@@ -571,119 +367,483 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
                 atomicOr(a.status, kErrBadSequences);
                 write_frame_header(slot, w);
                 a.sec_off[b] = 0;  // raw frame
+                plan->nlit = 0u;
             }
             __syncthreads();
             continue;
         }
         const uint32_t nlit = TLL + (w - TP);
-        // histogram, then the present bytes ranked by (count, byte)
-        for (uint32_t k = tid; k < nlit; k += kLitThreads) atomicAdd(&H.count[lit[k]], 1u);
-        __syncthreads();
-        uint32_t c = 0;
-        if (tid < 256u) {
-            c = H.count[tid];
-            if (c) {
-                uint32_t r = 0;
-                for (uint32_t s2 = 0; s2 < 256; ++s2) {
-                    const uint32_t cs = H.count[s2];
-                    r += (cs != 0u && (cs < c || (cs == c && s2 < tid))) ? 1u : 0u;
-                }
-                H.leaf[r] = static_cast<uint16_t>(tid);
-            }
+        const uint32_t rh = raw_lit_header_bytes(nlit);
+        uint8_t *dst = slot + fh + 3u + rh;
+        for (uint32_t k = tid; k < nlit; k += kLitThreads) {
+            const uint32_t x = lit[k];
+            dst[k] = static_cast<uint8_t>(x);
+            atomicAdd(&hist[x], 1u);
         }
-        const uint32_t nsym = __syncthreads_count(c != 0u);
         if (tid == 0) {
-            H.nsym = nsym;
-            H.huf_ok = nsym >= 2u ? huf_plan(H) : 0u;
-            H.seg = nlit < 1024u ? nlit : (nlit + 3u) / 4u;
-        }
-        __syncthreads();
-        const uint32_t nst_plan = nlit < 1024u ? 1u : 4u;
-        LitRun run{};
-        if (H.huf_ok) {  // exact bits of every run, and of every stream
-            run = lit_run(tid, nlit, nst_plan, H.seg);
-            uint32_t v = 0;
-            for (uint32_t k = run.lo; k < run.hi; ++k) v += H.len[lit[k]];
-            H.tbits[tid] = v;
-            uint32_t t = v;
-            for (uint32_t o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
-            if (lane == 0 && t) atomicAdd(&H.seg_bits[run.stream], t);
-        }
-        __syncthreads();
-        if (tid == 0) {
-            // choose the literal section and lay it out after the frame and block headers
-            const uint32_t L0 = fh + 3u;
-            const uint32_t raw_hdr = nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
-            uint32_t mode = 0, size = raw_hdr + nlit;  // 0 raw, 1 RLE, 2 Huffman
-            uint32_t hdr = 0, body = 0, nst = 0;
-            if (nsym == 1u) {
-                mode = 1;
-                size = raw_hdr + 1u;
-            } else if (H.huf_ok) {
-                nst = nlit < 1024u ? 1u : 4u;
-                uint32_t streams = 0;
-                for (uint32_t t = 0; t < nst; ++t) {
-                    H.stream_bytes[t] = (H.seg_bits[t] + 8u) >> 3;  // + end marker, rounded up
-                    streams += H.stream_bytes[t];
-                }
-                body = H.tree_bytes + (nst == 4u ? 6u : 0u) + streams;
-                hdr = nst == 1u ? 3u : (max(nlit, body) < 16384u ? 4u : 5u);
-                if ((nst == 1u && body >= 1024u) || hdr + body >= size) {
-                    nst = 0;
-                } else {
-                    mode = 2;
-                    size = hdr + body;
-                }
-            }
-            uint8_t *h = slot + L0;
             write_frame_header(slot, w);
-            if (mode == 2) {
-                uint64_t v;
-                if (hdr == 3u) v = 2u | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 14);
-                else if (hdr == 4u) v = 2u | (2u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 18);
-                else v = 2u | (3u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 22);
-                for (uint32_t i = 0; i < hdr; ++i) h[i] = static_cast<uint8_t>(v >> (8u * i));
-                for (uint32_t i = 0; i < H.tree_bytes; ++i) h[hdr + i] = H.tree[i];
-                uint32_t o = L0 + hdr + H.tree_bytes;
+            write_raw_lit_header(slot + fh + 3u, 0u, nlit);
+            a.sec_off[b] = fh + 3u + rh + nlit;
+            plan->nlit = nlit;
+        }
+        __syncthreads();
+        a.hist[static_cast<uint64_t>(b) * 256u + tid] = hist[tid];
+        __syncthreads();
+    }
+}
+
+// Bits into a byte buffer in shared memory, LSB first.
+struct SmemBits {
+    uint8_t *p;
+    uint32_t cap, pos, nbits;
+    uint64_t acc;
+    bool ovf;
+    __device__ void add(uint32_t v, uint32_t nb) {
+        acc |= static_cast<uint64_t>(v) << nbits;
+        nbits += nb;
+        while (nbits >= 8u) {
+            if (pos < cap) p[pos] = static_cast<uint8_t>(acc);
+            else ovf = true;
+            ++pos;
+            acc >>= 8;
+            nbits -= 8u;
+        }
+    }
+    __device__ void flush() {  // pad the last partial byte with zeros
+        if (nbits) add(0u, 8u - nbits);
+    }
+    __device__ void close() {  // end marker, then pad
+        add(1u, 1u);
+        flush();
+    }
+};
+
+constexpr uint32_t kPlanWarps = 4;
+
+struct PlanSmem {  // one per warp
+    uint32_t count[256];
+    uint32_t node[511];
+    uint32_t bl[64];
+    uint32_t start[16];
+    uint32_t cw[12];
+    uint32_t misc[4];  // [0] tree payload bytes (FSE), [1] ok
+    uint16_t leaf[256];
+    uint16_t anc[2][512];
+    uint16_t code[256];
+    uint8_t dep[2][512];
+    uint8_t len[256];
+    uint8_t tree[132];
+    uint8_t wts[256];
+    uint8_t st[256];
+    uint8_t fsym[64], fnb[64], fbase[64];
+    uint8_t fenc[12 * 64];
+};
+
+// FSE-compressed weights P.wts[0..N) into P.tree + 1 (lane 0, after the
+// parallel steps the caller ran); returns its size, or 0.
+__device__ uint32_t plan_fse_weights(PlanSmem &P, uint32_t N) {
+    const uint32_t lane = lane_id();
+    if (lane < 12u) P.cw[lane] = 0u;
+    __syncwarp();
+    for (uint32_t i = lane; i < N; i += 32u) atomicAdd(&P.cw[P.wts[i]], 1u);
+    __syncwarp();
+    int norm[12];
+    uint32_t distinct = 0;
+    int sum = 0, big = 0;
+    for (uint32_t s2 = 0; s2 < 12; ++s2) {
+        const uint32_t c = P.cw[s2];
+        distinct += c ? 1u : 0u;
+        norm[s2] = c ? max(1, static_cast<int>(c * 64u / N)) : 0;
+        sum += norm[s2];
+        if (norm[s2] > norm[big]) big = static_cast<int>(s2);
+    }
+    norm[big] += 64 - sum;
+    if (distinct < 2u || norm[big] <= 0) return 0;  // warp-uniform
+    if (lane == 0) {  // decoder table (no "less than 1" entries, so no high threshold)
+        uint32_t pos = 0;
+        for (uint32_t s2 = 0; s2 < 12; ++s2)
+            for (int c = 0; c < norm[s2]; ++c) {
+                P.fsym[pos] = static_cast<uint8_t>(s2);
+                pos = (pos + 43u) & 63u;  // step (64 >> 1) + (64 >> 3) + 3
+            }
+        uint32_t nxt[12];
+        for (uint32_t s2 = 0; s2 < 12; ++s2) nxt[s2] = static_cast<uint32_t>(norm[s2]);
+        for (uint32_t u = 0; u < 64; ++u) {
+            const uint32_t x = nxt[P.fsym[u]]++;
+            const uint32_t nb = 6u - highbit(x);
+            P.fnb[u] = static_cast<uint8_t>(nb);
+            P.fbase[u] = static_cast<uint8_t>((x << nb) - 64u);
+        }
+    }
+    __syncwarp();
+    for (uint32_t u = lane; u < 64u; u += 32u) {
+        const uint32_t b0 = P.fbase[u], e = b0 + (1u << P.fnb[u]);
+        for (uint32_t v = b0; v < e; ++v) P.fenc[P.fsym[u] * 64u + v] = static_cast<uint8_t>(u);
+    }
+    __syncwarp();
+    uint32_t size = 0;
+    if (lane == 0) {
+        // table description (RFC 8878 4.1.1)
+        SmemBits wr{P.tree + 1, 127u, 0u, 0u, 0ull, false};
+        wr.add(1u, 4u);  // accuracy 6
+        int remaining = 65, threshold = 64;
+        uint32_t nb = 7;
+        int lastw = 11;
+        while (norm[lastw] == 0) --lastw;
+        for (int s2 = 0; s2 <= lastw; ++s2) {
+            const int v = norm[s2] + 1, mx = (2 * threshold - 1) - remaining;
+            if (v < mx) wr.add(static_cast<uint32_t>(v), nb - 1u);
+            else if (v < threshold) wr.add(static_cast<uint32_t>(v), nb);
+            else wr.add(static_cast<uint32_t>(v + mx), nb);
+            remaining -= norm[s2];
+            while (remaining < threshold) {
+                --nb;
+                threshold >>= 1;
+            }
+            if (norm[s2] == 0) {
+                int z = 0;
+                while (s2 + 1 + z < lastw && norm[s2 + 1 + z] == 0) ++z;
+                s2 += z;
+                for (; z >= 3; z -= 3) wr.add(3u, 2u);
+                wr.add(static_cast<uint32_t>(z), 2u);
+            }
+        }
+        wr.flush();
+        // states: the last two weights pick theirs, the rest follow the chain
+        const uint32_t w1 = P.wts[N - 1], w2 = P.wts[N - 2];
+        uint32_t s_last = 64, s_prev = 64;
+        for (uint32_t u = 0; u < 64; ++u) {
+            if (s_last == 64 && P.fsym[u] == w1) s_last = u;
+            if (s_prev == 64 && P.fsym[u] == w2 && P.fnb[u] >= 1u) s_prev = u;
+        }
+        if (s_prev != 64) {
+            P.st[N - 1] = static_cast<uint8_t>(s_last);
+            P.st[N - 2] = static_cast<uint8_t>(s_prev);
+            for (int i = static_cast<int>(N) - 3; i >= 0; --i) P.st[i] = P.fenc[P.wts[i] * 64u + P.st[i + 2]];
+            SmemBits bs{P.tree + 1 + wr.pos, 127u > wr.pos ? 127u - wr.pos : 0u, 0u, 0u, 0ull, false};
+            for (int i = static_cast<int>(N) - 3; i >= 0; --i) {
+                const uint32_t sti = P.st[i];
+                bs.add(P.st[i + 2] - P.fbase[sti], P.fnb[sti]);
+            }
+            bs.add(P.st[1], 6u);
+            bs.add(P.st[0], 6u);
+            bs.close();
+            if (!wr.ovf && !bs.ovf && wr.pos + bs.pos <= 127u) size = wr.pos + bs.pos;
+        }
+    }
+    return __shfl_sync(kFull, size, 0);
+}
+
+// One warp per window: the Huffman code of the window's literals.
+__global__ void __launch_bounds__(32 * kPlanWarps) zenc_huf_plan_kernel(ZencArgs a) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    PlanSmem &P = reinterpret_cast<PlanSmem *>(smem_raw)[wid];
+    for (uint32_t b = blockIdx.x * kPlanWarps + wid; b < a.num_windows; b += gridDim.x * kPlanWarps) {
+        PlanRec *plan = reinterpret_cast<PlanRec *>(a.plan + static_cast<uint64_t>(b) * kZencPlanBytes);
+        const uint32_t nlit = a.sec_off[b] ? plan->nlit : 0u;
+        uint32_t mode = 0;
+        if (nlit) {
+            const uint32_t *hist = a.hist + static_cast<uint64_t>(b) * 256u;
+            // present bytes: ranks by (count, byte); lane l holds bytes 8l .. 8l+7
+            uint32_t c8[8];
+            uint32_t present = 0, top = 0;
+            for (uint32_t i = 0; i < 8; ++i) {
+                c8[i] = hist[lane * 8u + i];
+                P.count[lane * 8u + i] = c8[i];
+                if (c8[i]) {
+                    ++present;
+                    top = lane * 8u + i;
+                }
+            }
+            uint32_t n = present;
+            for (uint32_t o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(kFull, n, o);
+            uint32_t last = top;
+            for (uint32_t o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(kFull, last, o));
+            __syncwarp();
+            if (n == 1u) {
+                mode = 1;
+                if (lane == 0) plan->rle = last;
+            } else {
+                uint32_t r8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                for (uint32_t s2 = 0; s2 < 256; ++s2) {
+                    const uint32_t cs = P.count[s2];
+                    if (!cs) continue;
+                    for (uint32_t i = 0; i < 8; ++i) {
+                        const uint32_t me = lane * 8u + i;
+                        r8[i] += (cs < c8[i] || (cs == c8[i] && s2 < me)) ? 1u : 0u;
+                    }
+                }
+                for (uint32_t i = 0; i < 8; ++i)
+                    if (c8[i]) P.leaf[r8[i]] = static_cast<uint16_t>(lane * 8u + i);
+                __syncwarp();
+                // two-queue Huffman construction (serial)
+                if (lane == 0) {
+                    for (uint32_t k = 0; k < n; ++k) P.node[k] = P.count[P.leaf[k]];
+                    uint32_t li = 0, ii = n, nxt = n;
+                    while (nxt < 2u * n - 1u) {
+                        uint32_t pick[2];
+                        for (uint32_t t = 0; t < 2; ++t) {
+                            if (li < n && (ii >= nxt || P.node[li] <= P.node[ii])) pick[t] = li++;
+                            else pick[t] = ii++;
+                        }
+                        P.node[nxt] = P.node[pick[0]] + P.node[pick[1]];
+                        P.anc[0][pick[0]] = P.anc[0][pick[1]] = static_cast<uint16_t>(nxt);
+                        ++nxt;
+                    }
+                }
+                __syncwarp();
+                // depths by pointer jumping (parent links, the root points to itself)
+                const uint32_t nn = 2u * n - 1u, root = nn - 1u;
+                for (uint32_t k = lane; k < nn; k += 32u) {
+                    if (k == root) P.anc[0][k] = static_cast<uint16_t>(root);
+                    P.dep[0][k] = k == root ? 0u : 1u;
+                }
+                if (lane < 64u) P.bl[lane] = 0u;
+                if (lane + 32u < 64u) P.bl[lane + 32u] = 0u;
+                __syncwarp();
+                uint32_t cur = 0;
+                for (uint32_t r = 0; r < 9; ++r) {
+                    for (uint32_t k = lane; k < nn; k += 32u) {
+                        const uint32_t an = P.anc[cur][k];
+                        P.dep[cur ^ 1u][k] = static_cast<uint8_t>(P.dep[cur][k] + P.dep[cur][an]);
+                        P.anc[cur ^ 1u][k] = P.anc[cur][an];
+                    }
+                    __syncwarp();
+                    cur ^= 1u;
+                }
+                for (uint32_t k = lane; k < n; k += 32u) atomicAdd(&P.bl[min(static_cast<uint32_t>(P.dep[cur][k]), 63u)], 1u);
+                __syncwarp();
+                if (lane == 0) {  // limit to 11 bits, keeping the code complete
+                    uint32_t maxlen = 0;
+                    for (uint32_t i = 0; i < 64; ++i)
+                        if (P.bl[i]) maxlen = i;
+                    for (uint32_t i = maxlen; i > kHufMaxBits; --i) {
+                        while (P.bl[i] > 0) {
+                            uint32_t j = i - 2u;
+                            while (P.bl[j] == 0) --j;
+                            P.bl[i] -= 2u;
+                            P.bl[i - 1] += 1u;
+                            P.bl[j + 1] += 2u;
+                            P.bl[j] -= 1u;
+                        }
+                    }
+                    uint32_t maxb = 0;
+                    for (uint32_t L = kHufMaxBits; L >= 1u && !maxb; --L)
+                        if (P.bl[L]) maxb = L;
+                    P.start[maxb] = 0;
+                    for (uint32_t L = maxb - 1; L >= 1u; --L) P.start[L] = (P.start[L + 1] + P.bl[L + 1]) >> 1;
+                    P.start[0] = maxb;
+                }
+                __syncwarp();
+                const uint32_t maxb = P.start[0];
+                // lengths: the longest codes to the least frequent bytes
+                for (uint32_t i = 0; i < 8; ++i) P.len[lane * 8u + i] = 0;
+                __syncwarp();
+                for (uint32_t k = lane; k < n; k += 32u) {
+                    uint32_t cum = 0;
+                    for (uint32_t L = kHufMaxBits; L >= 1u; --L) {
+                        if (k < cum + P.bl[L]) {
+                            P.len[P.leaf[k]] = static_cast<uint8_t>(L);
+                            break;
+                        }
+                        cum += P.bl[L];
+                    }
+                }
+                __syncwarp();
+                // canonical codes: start[L] + rank among the bytes of length L
+                uint32_t l8[8];
+                for (uint32_t i = 0; i < 8; ++i) l8[i] = P.len[lane * 8u + i];
+                for (uint32_t L = 1; L <= maxb; ++L) {
+                    uint32_t m = 0;
+                    for (uint32_t i = 0; i < 8; ++i) m += l8[i] == L ? 1u : 0u;
+                    uint32_t x = m;
+                    for (uint32_t dd = 1; dd < 32; dd <<= 1) {
+                        const uint32_t y = __shfl_up_sync(kFull, x, dd);
+                        if (lane >= dd) x += y;
+                    }
+                    uint32_t code = P.start[L] + x - m;
+                    for (uint32_t i = 0; i < 8; ++i)
+                        if (l8[i] == L) P.code[lane * 8u + i] = static_cast<uint16_t>(code++);
+                }
+                // weights of bytes 0 .. last-1 (the last one's is implied)
+                const uint32_t N = last;
+                for (uint32_t i = 0; i < 8; ++i) {
+                    const uint32_t s2 = lane * 8u + i;
+                    if (s2 < N) P.wts[s2] = l8[i] ? static_cast<uint8_t>(maxb + 1u - l8[i]) : 0u;
+                }
+                __syncwarp();
+                uint32_t tree_bytes = 0;
+                if (N <= 128u) {
+                    if (lane == 0) P.tree[0] = static_cast<uint8_t>(127u + N);
+                    for (uint32_t m2 = lane; m2 < (N + 1u) / 2u; m2 += 32u) {
+                        const uint32_t hi4 = P.wts[2u * m2], lo4 = 2u * m2 + 1u < N ? P.wts[2u * m2 + 1u] : 0u;
+                        P.tree[1u + m2] = static_cast<uint8_t>((hi4 << 4) | lo4);
+                    }
+                    tree_bytes = 1u + (N + 1u) / 2u;
+                } else {
+                    const uint32_t f = plan_fse_weights(P, N);
+                    if (f) {
+                        if (lane == 0) P.tree[0] = static_cast<uint8_t>(f);
+                        tree_bytes = 1u + f;
+                    }
+                }
+                __syncwarp();
+                if (tree_bytes) {
+                    mode = 2;
+                    for (uint32_t i = lane; i < 256u; i += 32u) {
+                        plan->len[i] = P.len[i];
+                        plan->code[i] = P.code[i];
+                    }
+                    for (uint32_t i = lane; i < tree_bytes; i += 32u) plan->tree[i] = P.tree[i];
+                    if (lane == 0) plan->tree_bytes = tree_bytes;
+                }
+            }
+        }
+        if (lane == 0) plan->mode = mode;
+        __syncwarp();
+    }
+}
+
+// Literal runs for the Huffman streams: with 4 streams, threads 64s .. 64s+63
+// split stream s; with one stream all threads split it.  Run j of a stream
+// covers [lo + j*size, lo + (j+1)*size); the stream's bits start with its last
+// literal, so the highest run comes first.
+struct LitRun {
+    uint32_t stream, j, group, lo, hi;
+};
+__device__ __forceinline__ LitRun lit_run(uint32_t tid, uint32_t nlit, uint32_t nstreams, uint32_t seg) {
+    LitRun r;
+    r.group = nstreams == 4u ? kLitThreads / 4u : kLitThreads;
+    r.stream = tid / r.group;
+    r.j = tid % r.group;
+    const uint32_t s_lo = r.stream * seg, s_hi = r.stream == nstreams - 1u ? nlit : s_lo + seg;
+    const uint32_t size = (s_hi - s_lo + r.group - 1u) / r.group;
+    r.lo = min(s_lo + r.j * size, s_hi);
+    r.hi = min(r.lo + size, s_hi);
+    return r;
+}
+
+struct WriteSmem {
+    uint8_t len[256];
+    uint16_t code[256];
+    uint32_t tbits[kLitThreads];
+    uint32_t seg_bits[4];
+    uint32_t stream_off[4], stream_bytes[4];
+    uint32_t mode, nstreams, seg;
+};
+constexpr uint32_t kWriteSmem = kMaxWindow + sizeof(WriteSmem);
+
+// Writes the codes of lit[hi-1] .. lit[lo] (in that order) at bit `bitpos` of
+// the 32-bit-word array `out`; `marker` appends the end-of-stream bit.  Words
+// this run shares with a neighbour are ORed in atomically, the others stored.
+__device__ void huf_write_run(const WriteSmem &H, const uint8_t *lit, uint32_t lo, uint32_t hi, uint32_t *out,
+                              uint64_t bitpos, bool marker) {
+    uint64_t word = bitpos >> 5;
+    uint32_t nb = static_cast<uint32_t>(bitpos & 31u);
+    uint64_t acc = 0;
+    bool first = true;
+    auto add = [&](uint32_t code, uint32_t len) {
+        acc |= static_cast<uint64_t>(code) << nb;
+        nb += len;
+        if (nb >= 32u) {
+            if (first) atomicOr(out + word, static_cast<uint32_t>(acc));
+            else out[word] = static_cast<uint32_t>(acc);
+            first = false;
+            ++word;
+            acc >>= 32;
+            nb -= 32u;
+        }
+    };
+    for (uint32_t k = hi; k > lo; --k) {
+        const uint32_t x = lit[k - 1];
+        add(H.code[x], H.len[x]);
+    }
+    if (marker) add(1u, 1u);
+    if (nb) atomicOr(out + word, static_cast<uint32_t>(acc));
+}
+
+// One CTA per window: the RLE or Huffman-coded literal section where it is
+// smaller than the raw one already in the slot.
+__global__ void __launch_bounds__(kLitThreads) zenc_huf_write_kernel(ZencArgs a) {
+    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow literal bytes, then WriteSmem
+    WriteSmem &H = *reinterpret_cast<WriteSmem *>(lit + kMaxWindow);
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    for (uint32_t b = blockIdx.x; b < a.num_windows; b += gridDim.x) {
+        const PlanRec *plan = reinterpret_cast<const PlanRec *>(a.plan + static_cast<uint64_t>(b) * kZencPlanBytes);
+        if (a.sec_off[b] == 0u) continue;  // raw frame (uniform over the CTA)
+        const uint32_t mode = plan->mode;
+        if (mode == 0u) continue;
+        const uint32_t w = win_size(a, b);
+        const uint32_t fh = frame_header_bytes(w), L0 = fh + 3u;
+        const uint32_t nlit = plan->nlit, rh = raw_lit_header_bytes(nlit);
+        uint8_t *slot = a.slots + static_cast<uint64_t>(b) * kZencSlot;
+        if (mode == 1u) {
+            if (tid == 0) {
+                write_raw_lit_header(slot + L0, 1u, nlit);
+                slot[L0 + rh] = static_cast<uint8_t>(plan->rle);
+                a.sec_off[b] = L0 + rh + 1u;
+            }
+            continue;
+        }
+        // Huffman: the literals back from the raw section, the code from the plan
+        const uint8_t *rawp = slot + L0 + rh;
+        for (uint32_t k = tid; k < nlit; k += kLitThreads) lit[k] = rawp[k];
+        H.len[tid] = plan->len[tid];
+        H.code[tid] = plan->code[tid];
+        if (tid < 4u) H.seg_bits[tid] = 0u;
+        __syncthreads();
+        const uint32_t nst = nlit < 1024u ? 1u : 4u;
+        const uint32_t seg = nlit < 1024u ? nlit : (nlit + 3u) / 4u;
+        const LitRun run = lit_run(tid, nlit, nst, seg);
+        uint32_t v = 0;
+        for (uint32_t k = run.lo; k < run.hi; ++k) v += H.len[lit[k]];
+        H.tbits[tid] = v;
+        uint32_t t = v;
+        for (uint32_t o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+        if (lane == 0 && t) atomicAdd(&H.seg_bits[run.stream], t);
+        __syncthreads();
+        if (tid == 0) {
+            const uint32_t tree_bytes = plan->tree_bytes;
+            uint32_t streams = 0;
+            for (uint32_t s2 = 0; s2 < nst; ++s2) {
+                H.stream_bytes[s2] = (H.seg_bits[s2] + 8u) >> 3;  // + end marker, rounded up
+                streams += H.stream_bytes[s2];
+            }
+            const uint32_t body = tree_bytes + (nst == 4u ? 6u : 0u) + streams;
+            const uint32_t hdr = nst == 1u ? 3u : (max(nlit, body) < 16384u ? 4u : 5u);
+            H.mode = 0;
+            if (!((nst == 1u && body >= 1024u) || hdr + body >= rh + nlit)) {
+                H.mode = 2;
+                H.nstreams = nst;
+                uint64_t hv;
+                if (hdr == 3u) hv = 2u | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 14);
+                else if (hdr == 4u) hv = 2u | (2u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 18);
+                else hv = 2u | (3u << 2) | (static_cast<uint64_t>(nlit) << 4) | (static_cast<uint64_t>(body) << 22);
+                uint8_t *h = slot + L0;
+                for (uint32_t i = 0; i < hdr; ++i) h[i] = static_cast<uint8_t>(hv >> (8u * i));
+                for (uint32_t i = 0; i < tree_bytes; ++i) h[hdr + i] = plan->tree[i];
+                uint32_t o = L0 + hdr + tree_bytes;
                 if (nst == 4u) {
-                    for (uint32_t t = 0; t < 3; ++t) {
-                        slot[o + 2 * t] = static_cast<uint8_t>(H.stream_bytes[t]);
-                        slot[o + 2 * t + 1] = static_cast<uint8_t>(H.stream_bytes[t] >> 8);
+                    for (uint32_t s2 = 0; s2 < 3; ++s2) {
+                        slot[o + 2 * s2] = static_cast<uint8_t>(H.stream_bytes[s2]);
+                        slot[o + 2 * s2 + 1] = static_cast<uint8_t>(H.stream_bytes[s2] >> 8);
                     }
                     o += 6u;
                 }
-                for (uint32_t t = 0; t < nst; ++t) {
-                    H.stream_off[t] = o;
-                    o += H.stream_bytes[t];
+                for (uint32_t s2 = 0; s2 < nst; ++s2) {
+                    H.stream_off[s2] = o;
+                    o += H.stream_bytes[s2];
                 }
-            } else {
-                const uint32_t type = mode;  // Raw_Literals_Block 0, RLE_Literals_Block 1
-                if (raw_hdr == 1u) {
-                    h[0] = static_cast<uint8_t>(type | (nlit << 3));
-                } else if (raw_hdr == 2u) {
-                    h[0] = static_cast<uint8_t>(type | (1u << 2) | ((nlit << 4) & 0xF0u));
-                    h[1] = static_cast<uint8_t>(nlit >> 4);
-                } else {
-                    h[0] = static_cast<uint8_t>(type | (3u << 2) | ((nlit << 4) & 0xF0u));
-                    h[1] = static_cast<uint8_t>(nlit >> 4);
-                    h[2] = static_cast<uint8_t>(nlit >> 12);
-                }
-                if (mode == 1u) h[raw_hdr] = lit[0];
+                a.sec_off[b] = o;
             }
-            H.mode = mode;
-            H.nstreams = nst;
-            a.sec_off[b] = L0 + size;
         }
         __syncthreads();
-        if (H.mode == 0u) {
-            const uint32_t raw_hdr = nlit < 32u ? 1u : (nlit < 4096u ? 2u : 3u);
-            uint8_t *dst = slot + fh + 3u + raw_hdr;
-            for (uint32_t k = tid; k < nlit; k += kLitThreads) dst[k] = lit[k];
-        } else if (H.mode == 2u) {
+        if (H.mode == 2u) {
             // The streams' bytes start at zero (runs OR their shared words in); the
-            // words that hold the last header bytes are kept.
+            // bytes of the headers before them are kept.
             const uint32_t s0b = H.stream_off[0];
-            const uint32_t s1b = H.stream_off[H.nstreams - 1u] + H.stream_bytes[H.nstreams - 1u];
+            const uint32_t s1b = H.stream_off[nst - 1u] + H.stream_bytes[nst - 1u];
             uint32_t *wslot = reinterpret_cast<uint32_t *>(slot);
             const uint32_t w0 = (s0b + 3u) >> 2, w1 = (s1b + 3u) >> 2;
             for (uint32_t k = s0b + tid; k < min(w0 * 4u, s1b); k += kLitThreads) slot[k] = 0;
@@ -693,8 +853,7 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             uint32_t off = 0;
             for (uint32_t j2 = run.j + 1u; j2 < run.group; ++j2) off += H.tbits[run.stream * run.group + j2];
             const uint64_t bitpos = 8ull * H.stream_off[run.stream] + off;
-            if (run.hi > run.lo || run.j == 0u)
-                huf_write_run(H, lit, run.lo, run.hi, wslot, bitpos, run.j == 0u);
+            if (run.hi > run.lo || run.j == 0u) huf_write_run(H, lit, run.lo, run.hi, wslot, bitpos, run.j == 0u);
         }
         __syncthreads();
     }
@@ -969,22 +1128,33 @@ ZencArgs args_of(const ZencLaunch &l) {
     a.sec_off = l.sec_off;
     a.fsize = l.fsize;
     a.raw = l.raw;
+    a.hist = l.hist;
+    a.plan = l.plan;
     a.status = l.status;
     return a;
 }
 
-unsigned long long g_lit_smem_set = 0, g_seq_smem_set = 0;
+unsigned long long g_lit_smem_set = 0, g_seq_smem_set = 0, g_plan_smem_set = 0, g_write_smem_set = 0;
 
 }  // namespace
 
 cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st) {
     if (l.num_windows == 0) return cudaSuccess;
     const ZencArgs a = args_of(l);
-    cudaError_t e = set_smem_once(zenc_literals_kernel, kLitSmem, g_lit_smem_set);
+    cudaError_t e = set_smem_once(zenc_literals_kernel, kMaxWindow, g_lit_smem_set);
     if (e != cudaSuccess) return e;
+    if ((e = set_smem_once(zenc_huf_plan_kernel, sizeof(PlanSmem) * kPlanWarps, g_plan_smem_set)) != cudaSuccess)
+        return e;
+    if ((e = set_smem_once(zenc_huf_write_kernel, kWriteSmem, g_write_smem_set)) != cudaSuccess) return e;
     int grid = l.num_sms * 3;
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    zenc_literals_kernel<<<grid, kLitThreads, kLitSmem, st>>>(a);
+    zenc_literals_kernel<<<grid, kLitThreads, kMaxWindow, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    uint32_t pgrid = (l.num_windows + kPlanWarps - 1) / kPlanWarps;
+    if (pgrid > static_cast<uint32_t>(l.num_sms * 5)) pgrid = static_cast<uint32_t>(l.num_sms * 5);
+    zenc_huf_plan_kernel<<<pgrid, 32 * kPlanWarps, sizeof(PlanSmem) * kPlanWarps, st>>>(a);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    zenc_huf_write_kernel<<<grid, kLitThreads, kWriteSmem, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = set_smem_once(zenc_sequences_kernel, sizeof(SeqSmem), g_seq_smem_set)) != cudaSuccess) return e;
     grid = l.num_sms * 3;
