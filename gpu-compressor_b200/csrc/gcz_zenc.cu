@@ -231,6 +231,29 @@ __device__ __forceinline__ void write_block_header(uint8_t *p, uint32_t type, ui
     p[2] = static_cast<uint8_t>(h >> 16);
 }
 
+// 4 bytes at p (any alignment) from global memory: the aligned words that
+// hold them, funnel-shifted; the second word is read only when p is unaligned,
+// so no word without a wanted byte is touched.
+__device__ __forceinline__ uint32_t load4(const uint8_t *p) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~static_cast<uintptr_t>(3));
+    const uint32_t sh = static_cast<uint32_t>(a & 3u) * 8u;
+    const uint32_t lo = __ldg(w);
+    return sh ? __funnelshift_r(lo, __ldg(w + 1), sh) : lo;
+}
+
+// The CTA copies n bytes from s to d (any alignments): aligned 32-bit stores
+// for the whole words of d, byte stores at its two ends.
+__device__ void cta_copy(uint8_t *d, const uint8_t *s, uint32_t n) {
+    const uint32_t tid = threadIdx.x, nt = blockDim.x;
+    const uint32_t head = min(n, (4u - static_cast<uint32_t>(reinterpret_cast<uintptr_t>(d) & 3u)) & 3u);
+    for (uint32_t k = tid; k < head; k += nt) d[k] = s[k];
+    const uint32_t nw = (n - head) >> 2;
+    uint32_t *dw = reinterpret_cast<uint32_t *>(d + head);
+    for (uint32_t k = tid; k < nw; k += nt) dw[k] = load4(s + head + 4u * k);
+    for (uint32_t k = head + 4u * nw + tid; k < n; k += nt) d[k] = s[k];
+}
+
 // ---------------------------------------------------------------- literals
 // The literal section is the smallest of: raw; RLE (one distinct byte);
 // Huffman-coded (RFC 8878 4.2), one stream below 1024 literals, else four.
@@ -355,7 +378,15 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             for (uint32_t i = i0; i < i1; ++i) {
                 const uint4 q = sq[i];
                 if (q.x > p + q.y) bad = 1u;  // match would reach before the window start
-                for (uint32_t k = 0; k < q.y; ++k) lit[d + k] = __ldg(src + p + k);
+                uint32_t k = 0;
+                for (; k + 4u <= q.y; k += 4u) {
+                    const uint32_t v = load4(src + p + k);
+                    lit[d + k] = static_cast<uint8_t>(v);
+                    lit[d + k + 1] = static_cast<uint8_t>(v >> 8);
+                    lit[d + k + 2] = static_cast<uint8_t>(v >> 16);
+                    lit[d + k + 3] = static_cast<uint8_t>(v >> 24);
+                }
+                for (; k < q.y; ++k) lit[d + k] = __ldg(src + p + k);
                 d += q.y;
                 p += q.y + q.z;
             }
@@ -1104,13 +1135,12 @@ __global__ void __launch_bounds__(256) zenc_compact_kernel(ZencArgs a, const uin
         const uint8_t *slot = a.slots + static_cast<uint64_t>(b) * kZencSlot;
         uint8_t *dst = out + o;
         if (!a.raw[b]) {
-            for (uint32_t k = tid; k < size; k += blockDim.x) dst[k] = slot[k];
+            cta_copy(dst, slot, static_cast<uint32_t>(size));
         } else {
             const uint32_t w = win_size(a, b);
             const uint32_t hl = frame_header_bytes(w) + 3u;
-            const uint8_t *src = a.src + static_cast<uint64_t>(b) * a.window;
-            for (uint32_t k = tid; k < hl; k += blockDim.x) dst[k] = slot[k];
-            for (uint32_t k = tid; k < w; k += blockDim.x) dst[hl + k] = __ldg(src + k);
+            cta_copy(dst, slot, hl);
+            cta_copy(dst + hl, a.src + static_cast<uint64_t>(b) * a.window, w);
         }
     }
 }
