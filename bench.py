@@ -166,6 +166,31 @@ def measured_traffic(workload, n):
         return json.load(f).get(workload)
 
 
+def cpu_library_baselines(data, kind, threads):
+    """Stock compressors at matched levels on the host cores, per 64 KiB window
+    like the match-finder levels: libzstd ZSTD_compress level 1 (Zstd) or
+    liblzma raw LZMA2 preset 9 (LZMA2), `threads` windows at a time.  nvCOMP is
+    not part of this image, so its L0 baseline is reported unavailable."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from gcz import codecs
+
+    wins = [data[o:o + 65536] for o in range(0, data.size, 65536)]
+    if kind == "zstd":
+        fn = lambda w: len(codecs.zstd_compress_level(w.tobytes(), 1))  # noqa: E731
+        name = "libzstd 1.5.5 ZSTD_compress level 1"
+    else:
+        fn = lambda w: len(codecs.lzma2_raw_compress(w.tobytes(), 9))  # noqa: E731
+        name = "liblzma 5.4.5 raw LZMA2 preset 9"
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        out = sum(ex.map(fn, wins))
+    dt = time.perf_counter() - t0
+    return {name: {"gbs": round(data.size / dt / 1e9, 4), "ratio": round(out / data.size, 4), "threads": threads,
+                   "sample_bytes": int(data.size)},
+            "nvcomp_zstd_l0": {"unavailable": "nvCOMP is not installed in this image"}}
+
+
 def cpu_oracle_time(data, depth, threads):
     from oracle import oracle as orc
 
@@ -251,13 +276,14 @@ def run_gcz(args):
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     traffic = measured_traffic(WORKLOAD, n)
 
-    cpu = None
+    cpu = libs = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = data[:256 << 20]
         dt, _ = cpu_oracle_time(sample, DEPTH, threads)
         cpu = {"value": round(sample.size / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"first 256 MiB of the same 1 GiB input (4096 windows), oracle/oracle.c on {threads} threads"}
+        libs = cpu_library_baselines(data[:256 << 20], "zstd", threads)
 
     total_launches = sum_over_ranks(dist, torch, all_launches)
     if rank == 0:
@@ -276,6 +302,7 @@ def run_gcz(args):
                          "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms_per_step": round(step_ms, 4),
                          "algorithmic_bytes_per_step": alg_bytes},
             "cpu_baseline": cpu,
+            "cpu_libraries": libs,
             "gpu_launches": int(total_launches),
             "clocks": clk.summary(),
         }
@@ -350,6 +377,19 @@ def run_lzma2(args):
         has_triage = h_has.clone()
         e2e_packed = e2e_run(h_packed.data_ptr())
         assert torch.equal(has_triage, h_has)
+    libs = l1 = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = data[:16 << 20]
+        libs = cpu_library_baselines(sample, "lzma2", threads)
+        # LZMA2 L1 end to end on the sample: GPU triage, then the preset-9 coder
+        # pool on every window with a match (compress_lzma2_custom.rs:570-597)
+        from gcz import formats
+        t0 = time.perf_counter()
+        blob = formats.compress_lzma2(sample.tobytes(), device_id=local, workers=threads)
+        dt = time.perf_counter() - t0
+        l1 = {"gbs": round(sample.size / dt / 1e9, 4), "ratio": round(len(blob) / sample.size, 4),
+              "coder_threads": threads, "sample_bytes": int(sample.size)}
     peak, peak_kind = peaks()
     step_ms = kern_ms / max(kern_launches, 1)
     alg_bytes = n + 4 * n + B  # input once + packed matches + has-match bytes
@@ -369,6 +409,7 @@ def run_lzma2(args):
                          "frac": round(achieved / peak, 4), "traffic": measured_traffic("lzma2_l1_1gib", n),
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "kernel_ms_per_step": round(step_ms, 4), "algorithmic_bytes_per_step": alg_bytes},
+            "cpu_libraries": libs, "lzma2_l1_nvlz_end_to_end": l1,
             "gpu_launches": int(all_launches), "clocks": clk.summary()}), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -509,22 +550,35 @@ def run_uneven(args):
         ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16,
                                          d_seqs.data_ptr(), cap, d_off.data_ptr(), st.cuda_stream)
 
-    for _ in range(3):
+    for _ in range(3):  # also sizes every buffer, so the captured launches allocate nothing
         step()
+    ctx.sync(st.cuda_stream)
+    # the whole batch as one CUDA graph (the launches of one match-find step)
+    cs = torch.cuda.Stream()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(cs):
+        with torch.cuda.graph(g, stream=cs):
+            ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16,
+                                             d_seqs.data_ptr(), cap, d_off.data_ptr(), cs.cuda_stream)
+    torch.cuda.synchronize()
+    g.replay()
+    torch.cuda.synchronize()
     ctx.sync(st.cuda_stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     for _ in range(args.steps):
-        step()
+        g.replay()
     e1.record(st)
     torch.cuda.synchronize()
+    ctx.sync(st.cuda_stream)
     ms = e0.elapsed_time(e1) / args.steps
     total = int(np.sum(sizes))
     print(json.dumps({
         "metric": "uneven-batch input GB/s per B200 (Zstd L1 match-find, one launch)",
         "value": round(total / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ms, 3),
         "config": {"workload": "uneven_batch", "files": args.files, "size_range": [4096, args.max_file],
-                   "input_bytes": total, "windows": int(wins.size), "mix": "Dirichlet(1,1,1) per file"}}), flush=True)
+                   "input_bytes": total, "windows": int(wins.size), "mix": "Dirichlet(1,1,1) per file",
+                   "launch": "one CUDA graph replay per step"}}), flush=True)
 
 
 def run_reference(args):

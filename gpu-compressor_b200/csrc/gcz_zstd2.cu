@@ -269,7 +269,11 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, Cand
         c0 = f - off;
     }
     uint32_t len;
-    if (lazy && f + 4u < size && bm_bit(bm, f + 1u)) {  // main match and lazy candidate together
+    // The lazy candidate at f+1 (zstd_compress.cu:278-307) is taken only when
+    // len2 > len + 1.  When it is the same match one byte on (cand(f+1) ==
+    // c0 + 1) it is exactly one byte shorter -- its 3 verified bytes include
+    // byte f+3 == c0+3, so the main match extends past 3 -- and is never taken.
+    if (lazy && f + 4u < size && bm_bit(bm, f + 1u) && cf1 != c0 + 1u) {  // main match and lazy candidate together
         uint32_t l1, l2;
         extend_pair(w, c0 + kMinMatch, f + kMinMatch, size - f - kMinMatch, cf1 + kMinMatch, f + 1u + kMinMatch,
                     size - f - 1u - kMinMatch, l1, l2);
