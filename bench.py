@@ -57,6 +57,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second (Poisson)")
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     ap.add_argument("--max-request", type=int, default=64 << 20, help="serving: largest request size")
+    ap.add_argument("--max-batch", type=int, default=256 << 20, help="serving: largest batch (bytes of input)")
     ap.add_argument("--files", type=int, default=4096, help="uneven: number of files")
     ap.add_argument("--max-file", type=int, default=8 << 20, help="uneven: largest file size")
     return ap.parse_args()
@@ -429,9 +430,9 @@ def run_serving(args):
     torch.cuda.set_device(local)
     ctx = gcz.Context(local)
     pool_n = 1 << 30
-    pool = torch.empty(pool_n, dtype=torch.uint8).pin_memory()
+    pool = torch.empty(pool_n, dtype=torch.uint8, pin_memory=True)
     gcz.gen_synthetic(5, pool_n, 8 << 20, out=pool.numpy())
-    srv = serving.Server(ctx, hbm_budget=120 * 10**9, max_batch_bytes=1 << 30)
+    srv = serving.Server(ctx, hbm_budget=120 * 10**9, max_batch_bytes=args.max_batch)
     rng = np.random.default_rng(11)
     count = int(args.rate * args.duration)
     gaps = rng.exponential(1.0 / args.rate, size=count)
@@ -443,25 +444,32 @@ def run_serving(args):
     pool_np = pool.numpy()
     q = []
     lock = threading.Condition()
-    # Output buffers: pinned, reused, one free list per power-of-two size class.
-    # Zstd results get room for n/16 + 1024 sequences (this input averages one
-    # sequence per ~50 bytes; a smaller real count never overflows it).
-    free = {}
-    free_lock = threading.Lock()
+    # Outputs go to one pinned ring, allocated in submission order and freed in
+    # completion order (the waiter completes requests in order); a full ring
+    # holds the submitter back.  Zstd results get room for n/16 + 1024
+    # sequences (this input averages one sequence per ~50 bytes).
+    ring_n = 4 << 30
+    ring = torch.empty(ring_n, dtype=torch.uint8, pin_memory=True).numpy()
+    rs = {"head": 0, "tail": 0}
+    ring_cv = threading.Condition()
 
-    def take(cls_bytes):
-        with free_lock:
-            lst = free.setdefault(cls_bytes, [])
-            if lst:
-                return lst.pop()
-        return torch.empty(cls_bytes, dtype=torch.uint8).pin_memory().numpy()
+    def ring_alloc(nbytes):
+        nbytes = (nbytes + 255) & ~255
+        with ring_cv:
+            h = rs["head"]
+            if h % ring_n + nbytes > ring_n:
+                h += ring_n - h % ring_n  # skip the ring's end
+            while h + nbytes - rs["tail"] > ring_n:
+                ring_cv.wait()
+            rs["head"] = h + nbytes
+            return h % ring_n, h + nbytes
 
-    def give(cls_bytes, buf):
-        with free_lock:
-            free[cls_bytes].append(buf)
+    def ring_free(end):
+        with ring_cv:
+            rs["tail"] = end
+            ring_cv.notify_all()
 
-    def cls(nbytes):
-        return 1 << max(12, int(nbytes - 1).bit_length())
+    lats = np.zeros(count)
 
     def waiter():
         i = 0
@@ -469,12 +477,25 @@ def run_serving(args):
             with lock:
                 while len(q) <= i:
                     lock.wait()
-                r, bufs = q[i]
+                r, end = q[i]
             srv.wait(r)
-            for c, b in bufs:
-                give(c, b)
+            lats[i] = r.latency_ms
+            ring_free(end)
             q[i] = None
             i += 1
+
+    # Warm-up outside the timed region: two largest batches of each kind, so both
+    # slots of the loop hold their device buffers at full size.
+    wn = min(args.max_batch, pool_n)
+    for kind in (serving.ZSTD, serving.LZMA2, serving.ZSTD, serving.LZMA2):
+        if kind == serving.ZSTD:
+            cap = wn // 16 + 1024
+            r = srv.submit(kind, pool_np[:wn], 16, out_a=ring[:cap * 16].view(np.uint32).reshape(cap, 4), cap=cap,
+                           out_b=ring[cap * 16:cap * 16 + (gcz.num_windows(wn) + 1) * 8].view(np.uint64))
+        else:
+            r = srv.submit(kind, pool_np[:wn], 32, out_b=ring[:gcz.num_windows(wn)], packed=False)
+        srv.wait(r)
+    base = srv.stats()
 
     wt = threading.Thread(target=waiter)
     wt.start()
@@ -489,30 +510,32 @@ def run_serving(args):
         nb = gcz.num_windows(n)
         if kinds[i] == serving.ZSTD:
             cap = n // 16 + 1024
-            ca, cb = cls(cap * 16), cls((nb + 1) * 8)
-            ba, bb = take(ca), take(cb)
+            na, nbb = cap * 16, ((nb + 1) * 8 + 255) & ~255
+            o, end = ring_alloc(na + nbb)
             r = srv.submit(serving.ZSTD, pool_np[offs[i]:offs[i] + n], int(depths[i]),
-                           out_a=ba.view(np.uint32)[:cap * 4].reshape(cap, 4), cap=cap, out_b=bb.view(np.uint64))
-            bufs = [(ca, ba), (cb, bb)]
+                           out_a=ring[o:o + na].view(np.uint32).reshape(cap, 4), cap=cap,
+                           out_b=ring[o + na:o + na + (nb + 1) * 8].view(np.uint64))
         else:
-            cb = cls(nb)
-            bb = take(cb)
-            r = srv.submit(serving.LZMA2, pool_np[offs[i]:offs[i] + n], 32, out_b=bb, packed=False)
-            bufs = [(cb, bb)]
+            o, end = ring_alloc(nb)
+            r = srv.submit(serving.LZMA2, pool_np[offs[i]:offs[i] + n], 32, out_b=ring[o:o + nb], packed=False)
         with lock:
-            q.append((r, bufs))
+            q.append((r, end))
             lock.notify()
     wt.join()
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
+    done_bytes = st["bytes"] - base["bytes"]
+    st["batches"] -= base["batches"]
+    st["completed"] -= base["completed"]
+    st["p50_ms"], st["p99_ms"] = float(np.percentile(lats, 50)), float(np.percentile(lats, 99))
     print(json.dumps({
-        "metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "value": round(st["bytes"] / wall / 1e9, 3),
+        "metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "value": round(done_bytes / wall / 1e9, 3),
         "unit": "GB/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic (seeded pool)",
         "config": {"workload": "serving_poisson", "rate_per_s": args.rate, "duration_s": args.duration,
                    "requests": count, "size_range": [4096, args.max_request], "mix": "70% zstd L1, 20% zstd L2, 10% lzma2 (has-match bytes only)",
-                   "outputs": "pinned, reused per size class", "offered_gbps": round(float(sizes.sum()) / args.duration / 1e9, 3), "hbm_budget_bytes": 120 * 10**9,
-                   "max_batch_bytes": 1 << 30},
+                   "outputs": "pinned 4 GiB ring, freed in completion order", "offered_gbps": round(float(sizes.sum()) / args.duration / 1e9, 3), "hbm_budget_bytes": 120 * 10**9,
+                   "max_batch_bytes": args.max_batch},
         "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3)},
         "batches": st["batches"], "completed": st["completed"], "wall_s": round(wall, 3)}), flush=True)
 

@@ -110,6 +110,11 @@ namespace {
 int ensure_dev(gcz_ctx *c, DevBuf &b, size_t bytes) {
     if (bytes == 0) bytes = 16;
     if (b.cap >= bytes) return GCZ_OK;
+    // Grow by at least a quarter, in 2 MiB steps: inputs that creep upwards
+    // (request batches) reallocate a few times, not on every new maximum --
+    // each cudaFree waits for the whole device.
+    if (b.cap) bytes = std::max(bytes, b.cap + b.cap / 4);
+    bytes = (bytes + (2u << 20) - 1) & ~static_cast<size_t>((2u << 20) - 1);
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.cap = 0;
