@@ -500,6 +500,17 @@ int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, 
     return GCZ_OK;
 }
 
+// Windows in the pipeline slice that starts at window b0 of nb.  Slices ramp
+// up from a quarter of `maxw` (the first copy-in and the last kernels and
+// copy-out overlap nothing, so short ones there shorten the whole call) to
+// maxw, and halve again over the last 2*maxw windows.
+size_t next_slice(size_t b0, size_t nb, size_t maxw) {
+    const size_t q = std::max<size_t>(maxw / 4, 1), rem = nb - b0;
+    size_t s = std::min(maxw, std::max(q, b0));
+    if (rem <= 2 * maxw) s = std::min(s, std::max(q, rem / 2));
+    return std::min(s, rem);
+}
+
 int drain_slots(gcz_ctx *c) {
     for (Slot &sl : c->slots) GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
     GCZ_CUDA(c, cudaStreamSynchronize(c->out_stream));
@@ -521,9 +532,9 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
     int r = GCZ_OK;
     uint64_t done = 0;  // sequences copied so far
     size_t k = 0;
-    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+    for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
         Slot &sl = c->slots[k & 1];
-        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sb = next_slice(b0, nb, c->slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
         sl.off = b0 * (size_t)kW;
@@ -599,9 +610,9 @@ extern "C" int gcz_zstd_compress_frames_gpu(gcz_ctx *c, const uint8_t *src, size
         return GCZ_OK;
     };
     size_t k = 0;
-    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+    for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
         Slot &sl = c->slots[k & 1];
-        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sb = next_slice(b0, nb, c->slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
         sl.off = b0 * (size_t)kW;
@@ -733,9 +744,9 @@ int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, u
         return GCZ_OK;
     };
     size_t k = 0;
-    for (size_t b0 = 0; b0 < nb && r == GCZ_OK; b0 += c->slice_windows, ++k) {
+    for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
         Slot &sl = c->slots[k & 1];
-        const size_t sb = std::min(nb - b0, (size_t)c->slice_windows);
+        sb = next_slice(b0, nb, c->slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
         sl.off = b0 * (size_t)kW;
