@@ -176,7 +176,10 @@ def cpu_library_baselines(data, kind, threads):
 
     from gcz import codecs
 
-    wins = [data[o:o + 65536] for o in range(0, data.size, 65536)]
+    if kind == "xz":
+        wins, kind = [], "lzma2"
+    else:
+        wins = [data[o:o + 65536] for o in range(0, data.size, 65536)]
     if kind == "zstd":
         fn = lambda w: len(codecs.zstd_compress_level(w.tobytes(), 1))  # noqa: E731
         name = "libzstd 1.5.5 ZSTD_compress level 1"
@@ -187,9 +190,40 @@ def cpu_library_baselines(data, kind, threads):
     with ThreadPoolExecutor(threads) as ex:
         out = sum(ex.map(fn, wins))
     dt = time.perf_counter() - t0
-    return {name: {"gbs": round(data.size / dt / 1e9, 4), "ratio": round(out / data.size, 4), "threads": threads,
-                   "sample_bytes": int(data.size)},
-            "nvcomp_zstd_l0": {"unavailable": "nvCOMP is not installed in this image"}}
+    res = {"nvcomp_zstd_l0": {"unavailable": "nvCOMP is not installed in this image"}}
+    if wins:
+        res[name] = {"gbs": round(data.size / dt / 1e9, 4), "ratio": round(out / data.size, 4), "threads": threads,
+                     "sample_bytes": int(data.size)}
+    if kind == "zstd":
+        # whole buffer, level 1, ZSTD_c_nbWorkers = threads (libzstd's own multithreading)
+        import ctypes
+        L = codecs.zstd()
+        L.ZSTD_compress2.argtypes = [ctypes.c_void_p] * 2 + [ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+        L.ZSTD_compress2.restype = ctypes.c_size_t
+        cctx = L.ZSTD_createCCtx()
+        L.ZSTD_CCtx_setParameter(cctx, 100, 1)  # ZSTD_c_compressionLevel
+        L.ZSTD_CCtx_setParameter(cctx, 400, threads)  # ZSTD_c_nbWorkers
+        dst = np.empty(L.ZSTD_compressBound(data.size), np.uint8)
+        t0 = time.perf_counter()
+        r = L.ZSTD_compress2(cctx, dst.ctypes.data, dst.size, data.ctypes.data, data.size)
+        dt = time.perf_counter() - t0
+        L.ZSTD_freeCCtx(cctx)
+        if not L.ZSTD_isError(r):
+            res["libzstd 1.5.5 whole buffer level 1, nbWorkers"] = {
+                "gbs": round(data.size / dt / 1e9, 4), "ratio": round(r / data.size, 4), "threads": threads,
+                "sample_bytes": int(data.size)}
+    else:
+        # liblzma's multithreaded stream encoder at preset 9 (xz 5.4.5 CLI), 8 MiB blocks
+        import shutil
+        if shutil.which("xz"):
+            t0 = time.perf_counter()
+            pr = subprocess.run(["xz", "-9", f"-T{threads}", "--block-size=8MiB", "-c"], input=data.tobytes(),
+                                capture_output=True, check=True)
+            dt = time.perf_counter() - t0
+            res["liblzma 5.4.5 stream encoder mt preset 9 (xz), 8 MiB blocks"] = {
+                "gbs": round(data.size / dt / 1e9, 4), "ratio": round(len(pr.stdout) / data.size, 4),
+                "threads": threads, "sample_bytes": int(data.size)}
+    return res
 
 
 def cpu_oracle_time(data, depth, threads):
@@ -285,6 +319,10 @@ def run_gcz(args):
         cpu = {"value": round(sample.size / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
                "sample": f"first 256 MiB of the same 1 GiB input (4096 windows), oracle/oracle.c on {threads} threads"}
         libs = cpu_library_baselines(data[:256 << 20], "zstd", threads)
+        small = data[:16 << 20]
+        dt1, _ = cpu_oracle_time(small, DEPTH, 1)
+        libs["oracle single thread"] = {"gbs": round(small.size / dt1 / 1e9, 4), "threads": 1,
+                                        "sample_bytes": int(small.size)}
 
     total_launches = sum_over_ranks(dist, torch, all_launches)
     if rank == 0:
@@ -383,6 +421,8 @@ def run_lzma2(args):
         threads = os.cpu_count() or 1
         sample = data[:16 << 20]
         libs = cpu_library_baselines(sample, "lzma2", threads)
+        mt = cpu_library_baselines(data[:64 << 20], "xz", threads)
+        libs.update({k: v for k, v in mt.items() if k.startswith("liblzma 5.4.5 stream")})
         # LZMA2 L1 end to end on the sample: GPU triage, then the preset-9 coder
         # pool on every window with a match (compress_lzma2_custom.rs:570-597)
         from gcz import formats
