@@ -80,10 +80,11 @@ class Context:
             raise GczError(rc, f"gcz_create(device={device}) failed")
         self._h = h
         self.device = int(device)
+        self._lib = L  # kept for close() during interpreter shutdown, when module globals are gone
 
     def close(self):
         if getattr(self, "_h", None):
-            L.gcz_destroy(self._h)
+            self._lib.gcz_destroy(self._h)
             self._h = None
 
     def __del__(self):

@@ -51,6 +51,7 @@ class Server:
         self._h = h
         self._lock = threading.Lock()
         self.ctx = ctx
+        self._lib = L  # kept for close() during interpreter shutdown
 
     @property
     def max_batch_bytes(self):
@@ -86,7 +87,7 @@ class Server:
 
     def close(self):
         if getattr(self, "_h", None):
-            L.gcz_server_destroy(self._h)
+            self._lib.gcz_server_destroy(self._h)
             self._h = None
 
     def __del__(self):
