@@ -281,10 +281,38 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
             const bool cont = lane > 0 && eq4 && ((eq4_bits >> (lane - 1)) & 1u) && c == c_prev + 1u;
             const uint32_t heads = __ballot_sync(kFull, !cont);
             const uint32_t head = 31u - static_cast<uint32_t>(__clz(heads & (lt | (1u << lane))));
+            // Run heads extend their own match for up to 16 more bytes; a head
+            // still matching after that is finished by the whole warp (128 bytes
+            // per iteration), so one long run does not leave 31 lanes idle.
             uint32_t ext = 0;
+            const uint32_t bound = size - q < kLzmaMaxMatch + 31u ? size - q : kLzmaMaxMatch + 31u;
+            bool pending = false;
             if (eq4 && !cont) {
-                const uint32_t bound = size - q < kLzmaMaxMatch + 31u ? size - q : kLzmaMaxMatch + 31u;
-                ext = extend_lane(win, c, q, 4u, bound);
+                const uint32_t lim1 = bound < 20u ? bound : 20u;
+                ext = extend_lane(win, c, q, 4u, lim1);
+                pending = ext == lim1 && lim1 < bound;
+            }
+            for (uint32_t pend = __ballot_sync(kFull, pending); pend; pend &= pend - 1u) {
+                const uint32_t hl = static_cast<uint32_t>(__ffs(pend)) - 1u;
+                const uint32_t hc = __shfl_sync(kFull, c, hl), hq = __shfl_sync(kFull, q, hl);
+                const uint32_t hb = __shfl_sync(kFull, bound, hl);
+                uint32_t len2 = __shfl_sync(kFull, ext, hl);
+                for (;;) {
+                    const uint32_t k = len2 + 4u * lane;
+                    uint32_t res = k;
+                    if (k < hb) {
+                        const uint32_t d = win.u32(hq + k) ^ win.u32(hc + k);
+                        const uint32_t fb = d ? (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3 : 4u;
+                        res = k + (fb < hb - k ? fb : hb - k);
+                    }
+                    const uint32_t sb = __ballot_sync(kFull, res < k + 4u);
+                    if (sb) {
+                        len2 = __shfl_sync(kFull, res, static_cast<uint32_t>(__ffs(sb)) - 1u);
+                        break;
+                    }
+                    len2 += 128u;
+                }
+                if (lane == hl) ext = len2;
             }
             const uint32_t ext_head = __shfl_sync(kFull, ext, head);
             uint32_t dist = 0, len = 0;
