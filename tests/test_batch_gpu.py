@@ -124,3 +124,30 @@ def test_sharded_single_rank_uses_gpu_context(ctx):
     p0, h0 = ctx.lzma2_match_find(data, 32)
     np.testing.assert_array_equal(p, p0)
     np.testing.assert_array_equal(h, h0)
+
+
+def test_host_pipeline_uneven_slices(ctx):
+    """1500 windows + a ragged tail: the host-buffer pipeline cuts ramped slices
+    of unequal size; results equal one device call and the oracle."""
+    import torch
+    import gcz
+
+    n = 1500 * 65536 + 777
+    data = gcz.gen_synthetic(91, n, 8 << 20)
+    seqs, off = ctx.zstd_match_find(data, 16)
+    d_in = torch.from_numpy(data).cuda()
+    cap = int(gcz.L.gcz_zstd_max_sequences(n))
+    d_seqs = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
+    d_off = torch.empty(gcz.num_windows(n) + 1, dtype=torch.int64, device="cuda")
+    ctx.zstd_match_find_device(d_in.data_ptr(), n, 16, d_seqs.data_ptr(), cap, d_off.data_ptr(), 0)
+    ctx.sync(0)
+    o_dev = d_off.cpu().numpy().astype(np.uint64)
+    np.testing.assert_array_equal(off, o_dev)
+    np.testing.assert_array_equal(seqs, d_seqs[:int(o_dev[-1])].cpu().numpy().view(np.uint32))
+    sub = data[:300 * 65536]
+    o_s, o_o = orc.zstd_sequences(sub, 16, threads=16)
+    np.testing.assert_array_equal(off[:301], o_o)
+    np.testing.assert_array_equal(seqs[:int(o_o[-1])], o_s)
+    packed, has = ctx.lzma2_match_find(data, 32)
+    np.testing.assert_array_equal(packed[:sub.size], orc.lzma_packed(sub, 32, threads=16))
+    np.testing.assert_array_equal(has, ctx.lzma2_triage(data, 32))
