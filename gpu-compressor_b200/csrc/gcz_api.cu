@@ -570,6 +570,7 @@ extern "C" int gcz_zstd_encode_frames_device(gcz_ctx *c, const uint8_t *d_src, s
     std::lock_guard<std::mutex> lk(c->mu);
     if ((n && (!d_src || !d_seqs || !d_seq_offsets || !d_out)) || !d_frame_offsets)
         return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_src)) return fail(c, GCZ_EINVAL, "d_src must be 16-byte aligned");
     if (nwin(n) > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "input too large");
     DeviceGuard g(c->device);
     cudaStream_t st = pick_stream(c, stream);

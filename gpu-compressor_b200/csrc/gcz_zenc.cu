@@ -102,12 +102,13 @@ struct CodeTables {
     }
 };
 
-// Encoder tables in shared memory: enc[s * size + v] = D | nbBits(D) << 8 | baseline(D) << 16
-// for the state D of symbol s whose interval holds decoder state v.
+// Encoder tables in shared memory: enc[s * size + v] = D | nbBits(D) << 6 | baseline(D) << 10
+// (16 bits: states and baselines are below 64, bit counts at most 6) for the
+// state D of symbol s whose interval holds decoder state v.
 struct FseEnc {
-    uint32_t ll[kLLSyms << kLLLog];
-    uint32_t ml[kMLSyms << kMLLog];
-    uint32_t of[kOFSyms << kOFLog];
+    uint16_t ll[kLLSyms << kLLLog];
+    uint16_t ml[kMLSyms << kMLLog];
+    uint16_t of[kOFSyms << kOFLog];
     uint8_t sym[64];
     uint8_t nbits[64];
     uint16_t base[64];
@@ -115,7 +116,7 @@ struct FseEnc {
 
 // Decoder table of a normalised distribution (RFC 8878 4.1.1: symbol spread,
 // then nbBits / baseline per state), turned into the encoder table above.
-__device__ void build_fse(FseEnc &t, const int8_t *norm, uint32_t nsym, uint32_t al, uint32_t *enc) {
+__device__ void build_fse(FseEnc &t, const int8_t *norm, uint32_t nsym, uint32_t al, uint16_t *enc) {
     const uint32_t size = 1u << al;
     if (threadIdx.x == 0) {
         const uint32_t mask = size - 1u, step = (size >> 1) + (size >> 3) + 3u;
@@ -148,7 +149,7 @@ __device__ void build_fse(FseEnc &t, const int8_t *norm, uint32_t nsym, uint32_t
     __syncthreads();
     for (uint32_t u = threadIdx.x; u < size; u += blockDim.x) {
         const uint32_t s = t.sym[u], nb = t.nbits[u], b = t.base[u];
-        const uint32_t e = u | (nb << 8) | (b << 16);
+        const uint16_t e = static_cast<uint16_t>(u | (nb << 6) | (b << 10));
         for (uint32_t v = b; v < b + (1u << nb); ++v) enc[s * size + v] = e;
     }
     __syncthreads();
@@ -307,13 +308,32 @@ __device__ void write_raw_lit_header(uint8_t *h, uint32_t type, uint32_t nlit) {
 
 // Gathers the literals of each window into shared memory (one CTA per
 // window), validates the sequences, writes frame header + raw literal
-// section into the slot and the histogram of the literal bytes.
-__global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) {
-    extern __shared__ __align__(16) uint8_t lit[];  // kMaxWindow literal bytes
-    __shared__ uint32_t warp_ll[kLitThreads / 32], warp_pos[kLitThreads / 32];
-    __shared__ uint32_t hist[256];
-    __shared__ uint32_t tot_ll, tot_pos, bad;
+// section into the slot and the histogram of the literal bytes.  The window
+// is staged into shared memory with 1-D bulk copies first, so the gather
+// copies shared memory to shared memory.
+constexpr uint32_t kGatherThreads = 512;
+
+struct GatherSmem {
+    uint8_t win[kMaxWindow + 64];  // staged window, zero padding after it
+    uint8_t lit[kMaxWindow];
+    // Byte counts: 4 copies per warp (by lane & 3), so the lanes that count
+    // the same frequent byte at once are spread over copies; summed at the end.
+    uint32_t hist[kGatherThreads / 32 * 4][256];
+    uint32_t warp_ll[kGatherThreads / 32], warp_pos[kGatherThreads / 32];
+    uint32_t tot_ll, tot_pos, bad, flags;
+    alignas(8) uint64_t bar;
+};
+
+__global__ void __launch_bounds__(kGatherThreads) zenc_literals_kernel(ZencArgs a) {
+    extern __shared__ __align__(128) uint8_t smem_raw[];
+    GatherSmem &S = *reinterpret_cast<GatherSmem *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+    uint32_t parity = 0;
+    if (tid == 0) {
+        mbar_init(&S.bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
     for (uint32_t b = blockIdx.x; b < a.num_windows; b += gridDim.x) {
         const uint32_t w = win_size(a, b);
         const uint8_t *src = a.src + static_cast<uint64_t>(b) * a.window;
@@ -323,8 +343,11 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
         uint8_t *slot = a.slots + static_cast<uint64_t>(b) * kZencSlot;
         PlanRec *plan = reinterpret_cast<PlanRec *>(a.plan + static_cast<uint64_t>(b) * kZencPlanBytes);
         const uint32_t fh = frame_header_bytes(w);
-        if (tid == 0) bad = ns > kZencMaxSeqs ? 1u : 0u;
-        hist[tid] = 0u;  // kLitThreads == 256
+        if (tid == 0) {
+            S.bad = ns > kZencMaxSeqs ? 1u : 0u;
+            S.flags = 0u;
+        }
+        for (uint32_t k = tid; k < kGatherThreads / 32 * 4 * 256; k += kGatherThreads) (&S.hist[0][0])[k] = 0u;
         __syncthreads();
         if (ns == 0u) {  // no sequences: the raw block is smaller
             if (tid == 0) {
@@ -335,65 +358,69 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             __syncthreads();
             continue;
         }
-        // Each thread owns a contiguous run of sequences; a block scan gives
-        // its first literal's output index and source position.
-        const uint32_t per = (ns + kLitThreads - 1) / kLitThreads;
-        const uint32_t i0 = min(tid * per, ns), i1 = min(i0 + per, ns);
+        if (wid == 0 && !stage_window(S.win, src, w, &S.bar, parity, a.status) && lane == 0) S.flags = 1u;
+        // Each warp owns a contiguous, equal share of the sequences and copies
+        // every literal run of its share with all 32 lanes, so one long run
+        // does not hold up the CTA.  First the warps' totals, then a scan over
+        // the warps gives each share's first literal index and source position.
+        constexpr uint32_t kW32 = kGatherThreads / 32;
+        const uint32_t per = (ns + kW32 - 1) / kW32;
+        const uint32_t i0 = min(wid * per, ns), i1 = min(i0 + per, ns);
         uint32_t sll = 0, spos = 0;
-        for (uint32_t i = i0; i < i1; ++i) {
+        for (uint32_t i = i0 + lane; i < i1; i += 32u) {
             const uint4 q = sq[i];
             // lengths bounded by the window, so the sums below cannot wrap
-            if (q.x == 0u || q.y > kMaxWindow || q.z < 3u || q.z > kMaxWindow) bad = 1u;
+            if (q.x == 0u || q.y > kMaxWindow || q.z < 3u || q.z > kMaxWindow) S.bad = 1u;
             sll += q.y;
             spos += q.y + q.z;
         }
-        uint32_t xll = sll, xpos = spos;
-        for (uint32_t d = 1; d < 32; d <<= 1) {
-            const uint32_t yl = __shfl_up_sync(kFull, xll, d), yp = __shfl_up_sync(kFull, xpos, d);
-            if (lane >= d) {
-                xll += yl;
-                xpos += yp;
+        for (uint32_t o = 16; o > 0; o >>= 1) {
+            sll += __shfl_xor_sync(kFull, sll, o);
+            spos += __shfl_xor_sync(kFull, spos, o);
+        }
+        if (lane == 0) {
+            S.warp_ll[wid] = sll;
+            S.warp_pos[wid] = spos;
+        }
+        __syncthreads();
+        if (S.flags) return;  // the bulk copy never completed: status recorded, every thread leaves
+        uint32_t d = 0, p = 0, TLL = 0, TP = 0;
+        for (uint32_t k = 0; k < kW32; ++k) {
+            if (k < wid) {
+                d += S.warp_ll[k];
+                p += S.warp_pos[k];
             }
+            TLL += S.warp_ll[k];
+            TP += S.warp_pos[k];
         }
-        if (lane == 31) {
-            warp_ll[wid] = xll;
-            warp_pos[wid] = xpos;
-        }
-        __syncthreads();
-        uint32_t base_ll = 0, base_pos = 0;
-        for (uint32_t k = 0; k < wid; ++k) {
-            base_ll += warp_ll[k];
-            base_pos += warp_pos[k];
-        }
-        if (tid == kLitThreads - 1) {
-            tot_ll = base_ll + xll;
-            tot_pos = base_pos + xpos;
-        }
-        uint32_t d = base_ll + xll - sll, p = base_pos + xpos - spos;
-        __syncthreads();
-        const uint32_t TP = tot_pos, TLL = tot_ll;
-        if (TP > w || bad) {
-            if (tid == 0) bad = 1u;
-        } else {
-            for (uint32_t i = i0; i < i1; ++i) {
-                const uint4 q = sq[i];
-                if (q.x > p + q.y) bad = 1u;  // match would reach before the window start
-                uint32_t k = 0;
-                for (; k + 4u <= q.y; k += 4u) {
-                    const uint32_t v = load4(src + p + k);
-                    lit[d + k] = static_cast<uint8_t>(v);
-                    lit[d + k + 1] = static_cast<uint8_t>(v >> 8);
-                    lit[d + k + 2] = static_cast<uint8_t>(v >> 16);
-                    lit[d + k + 3] = static_cast<uint8_t>(v >> 24);
+        if (!(TP > w || S.bad)) {
+            for (uint32_t ib = i0; ib < i1; ib += 32u) {
+                const uint32_t i = ib + lane;
+                uint4 q = make_uint4(0u, 0u, 0u, 0u);
+                if (i < i1) q = sq[i];
+                uint32_t xl = q.y, xp = q.y + q.z;  // inclusive scans over the batch
+                for (uint32_t o = 1; o < 32; o <<= 1) {
+                    const uint32_t yl = __shfl_up_sync(kFull, xl, o), yp = __shfl_up_sync(kFull, xp, o);
+                    if (lane >= o) {
+                        xl += yl;
+                        xp += yp;
+                    }
                 }
-                for (; k < q.y; ++k) lit[d + k] = __ldg(src + p + k);
-                d += q.y;
-                p += q.y + q.z;
+                const uint32_t my_d = d + xl - q.y, my_p = p + xp - q.y - q.z;
+                if (i < i1 && q.x > my_p + q.y) S.bad = 1u;  // match would reach before the window start
+                const uint32_t cnt = min(32u, i1 - ib);
+                for (uint32_t j = 0; j < cnt; ++j) {
+                    const uint32_t rd = __shfl_sync(kFull, my_d, j), rp = __shfl_sync(kFull, my_p, j);
+                    const uint32_t rl = __shfl_sync(kFull, q.y, j);
+                    for (uint32_t k = lane; k < rl; k += 32u) S.lit[rd + k] = S.win[rp + k];
+                }
+                d += __shfl_sync(kFull, xl, 31);
+                p += __shfl_sync(kFull, xp, 31);
             }
-            for (uint32_t k = tid; k < w - TP; k += kLitThreads) lit[TLL + k] = __ldg(src + TP + k);
+            for (uint32_t k = tid; k < w - TP; k += kGatherThreads) S.lit[TLL + k] = S.win[TP + k];
         }
         __syncthreads();
-        if (bad) {
+        if (S.bad) {
             if (tid == 0) {
                 atomicOr(a.status, kErrBadSequences);
                 write_frame_header(slot, w);
@@ -406,10 +433,11 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
         const uint32_t nlit = TLL + (w - TP);
         const uint32_t rh = raw_lit_header_bytes(nlit);
         uint8_t *dst = slot + fh + 3u + rh;
-        for (uint32_t k = tid; k < nlit; k += kLitThreads) {
-            const uint32_t x = lit[k];
+        uint32_t *myhist = S.hist[wid * 4u + (lane & 3u)];
+        for (uint32_t k = tid; k < nlit; k += kGatherThreads) {
+            const uint32_t x = S.lit[k];
             dst[k] = static_cast<uint8_t>(x);
-            atomicAdd(&hist[x], 1u);
+            atomicAdd(&myhist[x], 1u);
         }
         if (tid == 0) {
             write_frame_header(slot, w);
@@ -418,7 +446,11 @@ __global__ void __launch_bounds__(kLitThreads) zenc_literals_kernel(ZencArgs a) 
             plan->nlit = nlit;
         }
         __syncthreads();
-        a.hist[static_cast<uint64_t>(b) * 256u + tid] = hist[tid];
+        if (tid < 256u) {
+            uint32_t c = 0;
+            for (uint32_t h = 0; h < kGatherThreads / 32 * 4; ++h) c += S.hist[h][tid];
+            a.hist[static_cast<uint64_t>(b) * 256u + tid] = c;
+        }
         __syncthreads();
     }
 }
@@ -567,7 +599,7 @@ __device__ uint32_t plan_fse_weights(PlanSmem &P, uint32_t N) {
 
 // One warp per window: the Huffman code of the window's literals.
 __global__ void __launch_bounds__(32 * kPlanWarps) zenc_huf_plan_kernel(ZencArgs a) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
+    extern __shared__ __align__(128) uint8_t smem_raw[];
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     PlanSmem &P = reinterpret_cast<PlanSmem *>(smem_raw)[wid];
     for (uint32_t b = blockIdx.x * kPlanWarps + wid; b < a.num_windows; b += gridDim.x * kPlanWarps) {
@@ -592,7 +624,9 @@ __global__ void __launch_bounds__(32 * kPlanWarps) zenc_huf_plan_kernel(ZencArgs
             uint32_t last = top;
             for (uint32_t o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(kFull, last, o));
             __syncwarp();
-            if (n == 1u) {
+            if (n == 0u) {
+                // nothing counted although the window has literals: keep the raw section
+            } else if (n == 1u) {
                 mode = 1;
                 if (lane == 0) plan->rle = last;
             } else {
@@ -922,6 +956,7 @@ struct SeqSmem {
     CodeTables C;
     WarpSeq W[kSeqWarps];
 };
+static_assert(sizeof(SeqSmem) * 4 + 4 * 1024 <= 233472, "four sequence CTAs per SM");
 
 __device__ __forceinline__ void or_bits(uint32_t *buf, uint32_t bitpos, uint64_t v, uint32_t nb) {
     if (nb == 0u) return;
@@ -1009,19 +1044,19 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
         __syncwarp();
         if (lane < 3u) {  // the three FSE chains
             const uint32_t lg = lane == 2u ? kOFLog : kLLLog;
-            const uint32_t *enc = lane == 0u ? G.T.ll : (lane == 1u ? G.T.ml : G.T.of);
+            const uint16_t *enc = lane == 0u ? G.T.ll : (lane == 1u ? G.T.ml : G.T.of);
             const uint8_t *cd = S.code[lane];
             uint16_t *up = S.upd[lane];
             uint32_t j = 0;
             if (hi == ns) {  // last sequence: any state of its symbol, no bits
-                D = enc[static_cast<uint32_t>(cd[0]) << lg] & 0xFFu;
+                D = enc[static_cast<uint32_t>(cd[0]) << lg] & 63u;
                 up[0] = 0;
                 j = 1;
             }
             for (; j < len; ++j) {
                 const uint32_t e = enc[(static_cast<uint32_t>(cd[j]) << lg) + D];
-                up[j] = static_cast<uint16_t>((D - (e >> 16)) | (((e >> 8) & 0xFFu) << 8));
-                D = e & 0xFFu;
+                up[j] = static_cast<uint16_t>((D - (e >> 10)) | (((e >> 6) & 15u) << 8));
+                D = e & 63u;
             }
         }
         __syncwarp();
@@ -1094,7 +1129,7 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
 }
 
 __global__ void __launch_bounds__(32 * kSeqWarps) zenc_sequences_kernel(ZencArgs a) {
-    extern __shared__ __align__(16) uint8_t smem_raw[];
+    extern __shared__ __align__(128) uint8_t smem_raw[];
     SeqSmem &G = *reinterpret_cast<SeqSmem *>(smem_raw);
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     G.C.build();
@@ -1171,15 +1206,17 @@ unsigned long long g_lit_smem_set = 0, g_seq_smem_set = 0, g_plan_smem_set = 0, 
 cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st) {
     if (l.num_windows == 0) return cudaSuccess;
     const ZencArgs a = args_of(l);
-    cudaError_t e = set_smem_once(zenc_literals_kernel, kMaxWindow, g_lit_smem_set);
+    cudaError_t e = set_smem_once(zenc_literals_kernel, sizeof(GatherSmem), g_lit_smem_set);
     if (e != cudaSuccess) return e;
     if ((e = set_smem_once(zenc_huf_plan_kernel, sizeof(PlanSmem) * kPlanWarps, g_plan_smem_set)) != cudaSuccess)
         return e;
     if ((e = set_smem_once(zenc_huf_write_kernel, kWriteSmem, g_write_smem_set)) != cudaSuccess) return e;
-    int grid = l.num_sms * 3;
+    int grid = l.num_sms;  // one 512-thread CTA per SM (window + literals in shared memory)
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    zenc_literals_kernel<<<grid, kLitThreads, kMaxWindow, st>>>(a);
+    zenc_literals_kernel<<<grid, kGatherThreads, sizeof(GatherSmem), st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    grid = l.num_sms * 3;
+    if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
     uint32_t pgrid = (l.num_windows + kPlanWarps - 1) / kPlanWarps;
     if (pgrid > static_cast<uint32_t>(l.num_sms * 5)) pgrid = static_cast<uint32_t>(l.num_sms * 5);
     zenc_huf_plan_kernel<<<pgrid, 32 * kPlanWarps, sizeof(PlanSmem) * kPlanWarps, st>>>(a);
@@ -1187,7 +1224,7 @@ cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st) {
     zenc_huf_write_kernel<<<grid, kLitThreads, kWriteSmem, st>>>(a);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = set_smem_once(zenc_sequences_kernel, sizeof(SeqSmem), g_seq_smem_set)) != cudaSuccess) return e;
-    grid = l.num_sms * 3;
+    grid = l.num_sms * 4;  // 4 CTAs of ~56 KB per SM
     const uint32_t need = (l.num_windows + kSeqWarps - 1) / kSeqWarps;
     if (static_cast<uint32_t>(grid) > need) grid = static_cast<int>(need);
     zenc_sequences_kernel<<<grid, 32 * kSeqWarps, sizeof(SeqSmem), st>>>(a);

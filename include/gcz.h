@@ -285,7 +285,7 @@ int gcz_zstd_compress_frames(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_
  * gcz_zstd_encode_frames_device: the entropy stage alone, on device memory,
  * from the output of gcz_zstd_match_find_device (records + per-window
  * offsets): frames back to back in d_out, byte offsets of the frames in
- * d_frame_offsets[num_windows + 1].  Sequences that do not describe their
+ * d_frame_offsets[num_windows + 1].  d_src must be 16-byte aligned.  Sequences that do not describe their
  * window give GCZ_EINVAL at the next synchronising call (gcz_sync). */
 int gcz_zstd_compress_frames_gpu(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t level, uint8_t *out,
                                  size_t out_capacity, uint64_t *frame_sizes, size_t *out_size);
