@@ -65,7 +65,8 @@ struct gcz_ctx {
     uint32_t *d_status = nullptr;
     Scratch sc;      // scratch of the _device entry points
     Slot slots[2];   // host-buffer pipeline
-    uint32_t slice_windows = 1024;  // windows per pipeline slice (64 MiB)
+    uint32_t slice_windows = 1024;         // windows per pipeline slice (64 MiB)
+    uint32_t frames_slice_windows = 4096;  // ... of the GPU frames pipeline (256 MiB: its kernels want many windows)
     int staged = 1;
     int algo = 2;          // 1: fused single-warp kernels, 2: candidate sweep + second stage
     int parse_ctas = 3;    // second-stage CTAs per SM
@@ -418,6 +419,10 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->slice_windows = (uint32_t)value;
         return GCZ_OK;
     }
+    if (!strcmp(key, "frames_slice_windows") && value >= 1 && value <= (1L << 20)) {
+        c->frames_slice_windows = (uint32_t)value;
+        return GCZ_OK;
+    }
     if (!strcmp(key, "parse_ctas") && value >= 1 && value <= 8) {
         c->parse_ctas = (int)value;
         return GCZ_OK;
@@ -613,7 +618,7 @@ extern "C" int gcz_zstd_compress_frames_gpu(gcz_ctx *c, const uint8_t *src, size
     size_t k = 0;
     for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
         Slot &sl = c->slots[k & 1];
-        sb = next_slice(b0, nb, c->slice_windows);
+        sb = next_slice(b0, nb, c->frames_slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
         sl.off = b0 * (size_t)kW;
