@@ -17,8 +17,11 @@
 // of the three repeat offsets the decoder holds at that point.
 //
 // Kernels, per window:
-//   zenc_literals_kernel   (one CTA):    frame header, literal section (raw, RLE
-//                                        or Huffman-coded)
+//   zenc_literals_kernel   (one CTA):    window staged by bulk copy, literal
+//                                        gather, raw literal section, histogram
+//   zenc_huf_plan_kernel   (one warp):   Huffman code and tree description
+//   zenc_huf_write_kernel  (one CTA):    RLE or Huffman-coded literal section
+//                                        where that is smaller
 //   zenc_sequences_kernel  (one warp):   repeat-code pass, FSE chains, bitstream,
 //                                        block header, frame size
 //   zenc_compact_kernel    (one CTA):    frames back to back at scanned offsets
@@ -320,7 +323,7 @@ struct GatherSmem {
     // the same frequent byte at once are spread over copies; summed at the end.
     uint32_t hist[kGatherThreads / 32 * 4][256];
     uint32_t warp_ll[kGatherThreads / 32], warp_pos[kGatherThreads / 32];
-    uint32_t tot_ll, tot_pos, bad, flags;
+    uint32_t bad, flags;
     alignas(8) uint64_t bar;
 };
 
