@@ -14,6 +14,7 @@
 
 #include "gcz.h"
 #include "gcz_internal.h"
+#include "gcz_common.cuh"
 #include "gcz_kernels.h"
 
 namespace {
@@ -452,6 +453,30 @@ extern "C" int gcz_sync(gcz_ctx *c, void *stream) {
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard g(c->device);
     return read_status(c, pick_stream(c, stream));
+}
+
+namespace {
+// One CTA waits on an mbarrier that nothing will ever complete.  The wait is
+// bounded like every wait in the match finders; when it runs out the kernel
+// records the timeout in the status word and returns.
+__global__ void selftest_wait_kernel(uint32_t *status, uint32_t max_iter) {
+    __shared__ alignas(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        gcz::mbar_init(&bar, 1);
+        gcz::fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !gcz::mbar_wait(&bar, 0u, max_iter)) atomicOr(status, gcz::kErrTmaTimeout);
+}
+}  // namespace
+
+extern "C" int gcz_selftest_wait_timeout(gcz_ctx *c, uint32_t max_iterations) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    selftest_wait_kernel<<<1, 32, 0, c->stream>>>(c->d_status, max_iterations);
+    GCZ_CUDA(c, cudaGetLastError());
+    return read_status(c, c->stream);
 }
 
 // =========================================================================== Zstd

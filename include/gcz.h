@@ -295,6 +295,13 @@ int gcz_zstd_encode_frames_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, 
                                   const uint64_t *d_seq_offsets, uint8_t *d_out, size_t out_capacity,
                                   uint64_t *d_frame_offsets, void *stream);
 
+/* Self-test of the error path (no counterpart in the reference): one CTA waits
+ * on an mbarrier that nothing completes, with the same kind of bounded wait
+ * the kernels use around their bulk copies; the wait runs out after
+ * max_iterations tries and the kernel records it, so this returns GCZ_EDEVICE
+ * and the context stays usable.  No fault, trap or hang is involved. */
+int gcz_selftest_wait_timeout(gcz_ctx *ctx, uint32_t max_iterations);
+
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this
  * context launches is bracketed by CUDA events on its own launch stream.
  * gcz_profile_stop synchronises those events and returns the summed device
