@@ -278,8 +278,8 @@ int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st)
 // frames back to back in d_out, frame offsets (nwin+1) in d_frame_offsets.
 int zenc_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, const void *d_seqs,
               const uint64_t *d_seq_offsets, uint8_t *d_out, uint64_t out_capacity, uint64_t *d_frame_offsets,
-              cudaStream_t st) {
-    const size_t nb = nwin(n);
+              cudaStream_t st, const gcz::WinDesc *wins = nullptr, size_t nbw = 0) {
+    const size_t nb = wins ? nbw : nwin(n);
     int r;
     if ((r = ensure_dev(c, sc.zslots, nb * (size_t)gcz::kZencSlot)) != GCZ_OK) return r;
     if ((r = ensure_dev(c, sc.zovs, nb * (size_t)gcz::kZencMaxSeqs * 4)) != GCZ_OK) return r;
@@ -301,6 +301,7 @@ int zenc_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, const voi
     l.hist = reinterpret_cast<uint32_t *>(l.plan + nb * (size_t)gcz::kZencPlanBytes);
     l.status = c->d_status;
     l.num_sms = c->num_sms;
+    l.wins = wins;
     GCZ_CUDA(c, gcz::launch_zenc(l, st));
     GCZ_CUDA(c, gcz::launch_scan_counts(l.fsize, (uint32_t)nb, d_frame_offsets, st));
     GCZ_CUDA(c, gcz::launch_zenc_compact(l, d_frame_offsets, d_out, out_capacity, st));
@@ -1005,6 +1006,81 @@ extern "C" int gcz_zstd_match_find_files(gcz_ctx *c, const uint8_t *const *srcs,
         GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
         return read_status(c, sl.st);
     }
+}
+
+extern "C" int gcz_zstd_encode_frames_batch_device(gcz_ctx *c, const uint8_t *d_slab, uint64_t slab_bytes,
+                                                   const gcz_window *d_windows, uint32_t num_windows,
+                                                   const gcz_zstd_sequence *d_seqs, const uint64_t *d_seq_offsets,
+                                                   uint8_t *d_out, size_t out_capacity, uint64_t *d_frame_offsets,
+                                                   void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!d_frame_offsets || (num_windows && (!d_slab || !d_windows || !d_seqs || !d_seq_offsets || !d_out)))
+        return fail(c, GCZ_EINVAL, "null pointer");
+    if (!aligned16(d_slab)) return fail(c, GCZ_EINVAL, "d_slab must be 16-byte aligned");
+    DeviceGuard g(c->device);
+    cudaStream_t st = pick_stream(c, stream);
+    if (num_windows == 0) {
+        GCZ_CUDA(c, cudaMemsetAsync(d_frame_offsets, 0, 8, st));
+        return GCZ_OK;
+    }
+    return zenc_core(c, c->sc, d_slab, slab_bytes, d_seqs, d_seq_offsets, d_out, out_capacity, d_frame_offsets, st,
+                     reinterpret_cast<const gcz::WinDesc *>(d_windows), num_windows);
+}
+
+extern "C" int gcz_zstd_compress_files_gpu(gcz_ctx *c, const uint8_t *const *srcs, const size_t *sizes, size_t count,
+                                           uint32_t level, uint8_t *out, size_t out_capacity, uint64_t *frame_sizes,
+                                           size_t *out_size) {
+    if (!c) return GCZ_EINVAL;
+    if ((count && (!srcs || !sizes)) || !out_size) return fail(c, GCZ_EINVAL, "null pointer");
+    *out_size = 0;
+    const size_t nb = gcz_batch_num_windows(sizes, count);
+    if (nb > 0xFFFFFFFFu) return fail(c, GCZ_EINVAL, "too many windows");
+    if (nb && (!out || !frame_sizes)) return fail(c, GCZ_EINVAL, "null pointer");
+    std::vector<uint64_t> foff(count);
+    std::vector<gcz_window> wins(nb);
+    uint64_t slab = 0;
+    gcz_batch_layout(sizes, count, foff.data(), wins.data(), &slab);
+    if (nb == 0) return GCZ_OK;
+    const uint32_t depth = gcz_zstd_search_depth_for_level(level);
+    int r;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    Slot &sl = c->slots[0];
+    size_t cap = 0, fbound = 0;
+    for (size_t i = 0; i < count; i++) {
+        cap += gcz_zstd_max_sequences(sizes[i]);
+        fbound += gcz_zstd_frames_bound(sizes[i]);
+    }
+    if ((r = ensure_dev(c, sl.in, slab + 64)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sl.lz_has, nb * sizeof(gcz_window))) != GCZ_OK) return r;  // window table
+    if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sl.frames, fbound)) != GCZ_OK) return r;
+    if ((r = ensure_dev(c, sl.foff, (nb + 1) * 8)) != GCZ_OK) return r;
+    if ((r = ensure_host(c, sl.h_foff, (nb + 1) * 8)) != GCZ_OK) return r;
+    uint8_t *slab_p = static_cast<uint8_t *>(sl.in.p);
+    for (size_t i = 0; i < count; i++)
+        if (sizes[i]) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + foff[i], srcs[i], sizes[i], cudaMemcpyHostToDevice, sl.st));
+    GCZ_CUDA(c, cudaMemcpyAsync(sl.lz_has.p, wins.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, sl.st));
+    const gcz::WinDesc *dw = static_cast<const gcz::WinDesc *>(sl.lz_has.p);
+    uint64_t *d_off = static_cast<uint64_t *>(sl.offsets.p);
+    if ((r = zstd_device_core(c, sl.sc, slab_p, slab, depth, sl.seqs.p, cap, d_off, sl.st, dw, nb)) != GCZ_OK) return r;
+    if ((r = zenc_core(c, sl.sc, slab_p, slab, sl.seqs.p, d_off, static_cast<uint8_t *>(sl.frames.p), fbound,
+                       static_cast<uint64_t *>(sl.foff.p), sl.st, dw, nb)) != GCZ_OK)
+        return r;
+    GCZ_CUDA(c, cudaMemcpyAsync(sl.h_foff.p, sl.foff.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+    GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+    if ((r = read_status(c, sl.st)) != GCZ_OK) return r;
+    const uint64_t *ho = static_cast<const uint64_t *>(sl.h_foff.p);
+    const uint64_t total = ho[nb];
+    if (total > out_capacity)
+        return fail(c, GCZ_ECAPACITY, "frames need %llu bytes, capacity %zu", (unsigned long long)total, out_capacity);
+    GCZ_CUDA(c, cudaMemcpyAsync(out, sl.frames.p, total, cudaMemcpyDeviceToHost, sl.st));
+    for (size_t i = 0; i < nb; ++i) frame_sizes[i] = ho[i + 1] - ho[i];
+    GCZ_CUDA(c, cudaStreamSynchronize(sl.st));
+    *out_size = total;
+    return GCZ_OK;
 }
 
 // =========================================================================== serving

@@ -101,6 +101,7 @@ struct ZencLaunch {
     uint8_t *plan;                // num_windows * kZencPlanBytes
     uint32_t *status;
     int num_sms;
+    const WinDesc *wins = nullptr;  // optional window table (16-byte-aligned offsets)
 };
 cudaError_t launch_zenc(const ZencLaunch &l, cudaStream_t st);
 cudaError_t launch_zenc_compact(const ZencLaunch &l, const uint64_t *frame_offsets, uint8_t *out, uint64_t capacity,

@@ -205,11 +205,17 @@ struct ZencArgs {
     uint32_t *hist;            // 256 literal-byte counts per window
     uint8_t *plan;             // kZencPlanBytes per window
     uint32_t *status;
+    const WinDesc *wins;       // optional window table (null: windows at b * window)
 };
 
 __device__ __forceinline__ uint32_t win_size(const ZencArgs &a, uint32_t b) {
+    if (a.wins) return a.wins[b].size;
     const uint64_t s = static_cast<uint64_t>(b) * a.window;
     return static_cast<uint32_t>(a.n - s < a.window ? a.n - s : a.window);
+}
+// First byte of window b: at b * window, or where the window table puts it.
+__device__ __forceinline__ const uint8_t *win_src(const ZencArgs &a, uint32_t b) {
+    return a.src + (a.wins ? a.wins[b].offset : static_cast<uint64_t>(b) * a.window);
 }
 __device__ __forceinline__ uint32_t frame_header_bytes(uint32_t w) { return 4u + 1u + (w < 256u ? 1u : 2u); }
 
@@ -339,7 +345,7 @@ __global__ void __launch_bounds__(kGatherThreads) zenc_literals_kernel(ZencArgs 
     __syncthreads();
     for (uint32_t b = blockIdx.x; b < a.num_windows; b += gridDim.x) {
         const uint32_t w = win_size(a, b);
-        const uint8_t *src = a.src + static_cast<uint64_t>(b) * a.window;
+        const uint8_t *src = win_src(a, b);
         const uint64_t s0 = a.seq_offsets[b];
         const uint32_t ns = static_cast<uint32_t>(a.seq_offsets[b + 1] - s0);
         const uint4 *sq = a.seqs + s0;
@@ -1178,7 +1184,7 @@ __global__ void __launch_bounds__(256) zenc_compact_kernel(ZencArgs a, const uin
             const uint32_t w = win_size(a, b);
             const uint32_t hl = frame_header_bytes(w) + 3u;
             cta_copy(dst, slot, hl);
-            cta_copy(dst + hl, a.src + static_cast<uint64_t>(b) * a.window, w);
+            cta_copy(dst + hl, win_src(a, b), w);
         }
     }
 }
@@ -1199,6 +1205,7 @@ ZencArgs args_of(const ZencLaunch &l) {
     a.hist = l.hist;
     a.plan = l.plan;
     a.status = l.status;
+    a.wins = l.wins;
     return a;
 }
 

@@ -228,6 +228,37 @@ class Context:
                                                    sizes.ctypes.data, ctypes.byref(used)))
         return out[:used.value], sizes[:num_windows(n)]
 
+    def zstd_compress_files_gpu(self, files, level=1):
+        """GPU frames of many host files in one launch of each kernel: a list
+        with, per file, the list of its frames (one per 64 KiB window)."""
+        arrs = [_u8(f) for f in files]
+        k = len(arrs)
+        sizes = (ctypes.c_size_t * k)(*[a.size for a in arrs])
+        ptrs = (ctypes.c_void_p * k)(*[a.ctypes.data if a.size else None for a in arrs])
+        nb = int(L.gcz_batch_num_windows(sizes, k))
+        bound = sum(int(L.gcz_zstd_frames_bound(a.size)) for a in arrs)
+        out = np.empty(max(bound, 1), np.uint8)
+        fs = np.zeros(max(nb, 1), np.uint64)
+        used = ctypes.c_size_t()
+        self._check(L.gcz_zstd_compress_files_gpu(self._h, ptrs, sizes, k, level, out.ctypes.data, out.size,
+                                                  fs.ctypes.data, ctypes.byref(used)))
+        res, pos, w = [], 0, 0
+        for a in arrs:
+            frames = []
+            for _ in range(num_windows(a.size)):
+                s = int(fs[w])
+                frames.append(out[pos:pos + s].tobytes())
+                pos += s
+                w += 1
+            res.append(frames)
+        return res
+
+    def zstd_encode_frames_batch_device(self, d_slab, slab_bytes, d_windows, num_windows, d_seqs, d_seq_offsets,
+                                        d_out, out_capacity, d_frame_offsets, stream=None):
+        self._check(L.gcz_zstd_encode_frames_batch_device(self._h, d_slab, slab_bytes, d_windows, num_windows, d_seqs,
+                                                          d_seq_offsets, d_out, out_capacity, d_frame_offsets,
+                                                          _stream(stream)))
+
     def zstd_encode_frames_device(self, d_src, n, d_seqs, d_seq_offsets, d_out, out_capacity, d_frame_offsets,
                                   stream=None):
         self._check(L.gcz_zstd_encode_frames_device(self._h, d_src, n, d_seqs, d_seq_offsets, d_out, out_capacity,

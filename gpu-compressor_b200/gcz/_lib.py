@@ -63,6 +63,8 @@ SIGNATURES = {
     "gcz_zstd_compress_frames_gpu": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp, ctypes.POINTER(_sz)]),
     "gcz_zstd_encode_frames_device": (_i, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp]),
     "gcz_selftest_wait_timeout": (_i, [_vp, _u32]),
+    "gcz_zstd_encode_frames_batch_device": (_i, [_vp, _vp, _u64, _vp, _u32, _vp, _vp, _vp, _sz, _vp, _vp]),
+    "gcz_zstd_compress_files_gpu": (_i, [_vp, _vp, _vp, _sz, _u32, _vp, _sz, _vp, ctypes.POINTER(_sz)]),
     "gcz_profile_start": (_i, [_vp]),
     "gcz_profile_stop": (_i, [_vp, ctypes.POINTER(_d), ctypes.POINTER(_u64), ctypes.POINTER(_u64)]),
     "gcz_gen_synthetic": (None, [_u64, _vp, _u64, _u64, _d, _d, _d]),

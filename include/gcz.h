@@ -295,6 +295,24 @@ int gcz_zstd_encode_frames_device(gcz_ctx *ctx, const uint8_t *d_src, size_t n, 
                                   const uint64_t *d_seq_offsets, uint8_t *d_out, size_t out_capacity,
                                   uint64_t *d_frame_offsets, void *stream);
 
+/* GPU frames for a batch of files (window table as for
+ * gcz_zstd_match_find_batch_device): the entropy stage over the records and
+ * per-window offsets of gcz_zstd_match_find_batch_device, frames of all
+ * windows back to back in window order (file by file), byte offsets in
+ * d_frame_offsets[num_windows + 1].  gcz_zstd_compress_files_gpu is the
+ * host form: k host files in, their frames back to back in `out` and one
+ * size per window in frame_sizes (gcz_batch_num_windows entries); one
+ * launch of each kernel covers every file.  out_capacity >= the sum of
+ * gcz_zstd_frames_bound(sizes[i]) always suffices.  Each frame equals the
+ * one gcz_zstd_compress_frames_gpu gives for that window. */
+int gcz_zstd_encode_frames_batch_device(gcz_ctx *ctx, const uint8_t *d_slab, uint64_t slab_bytes,
+                                        const gcz_window *d_windows, uint32_t num_windows,
+                                        const gcz_zstd_sequence *d_seqs, const uint64_t *d_seq_offsets,
+                                        uint8_t *d_out, size_t out_capacity, uint64_t *d_frame_offsets, void *stream);
+int gcz_zstd_compress_files_gpu(gcz_ctx *ctx, const uint8_t *const *srcs, const size_t *sizes, size_t count,
+                                uint32_t level, uint8_t *out, size_t out_capacity, uint64_t *frame_sizes,
+                                size_t *out_size);
+
 /* Self-test of the error path (no counterpart in the reference): one CTA waits
  * on an mbarrier that nothing completes, with the same kind of bounded wait
  * the kernels use around their bulk copies; the wait runs out after

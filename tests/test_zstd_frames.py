@@ -165,3 +165,48 @@ def test_gpu_frames_empty_and_capacity(ctx):
     rc = gcz.L.gcz_zstd_compress_frames_gpu(ctx.handle, data.ctypes.data, data.size, 1, out.ctypes.data, out.size,
                                             fs.ctypes.data, ctypes.byref(used))
     assert rc == -4 and used.value == 0
+
+
+@pytest.mark.gpu
+def test_gpu_frames_for_file_batches(ctx):
+    """Many files in one launch of each kernel (window table): every file's
+    frames equal the ones the single-buffer call gives for it and decode with
+    stock libzstd; the device batch call gives the same bytes."""
+    import torch
+    import gcz
+    from gcz import codecs
+
+    rng = np.random.default_rng(8)
+    sizes = [0, 1, 300, 65535, 65536, 65537, (3 << 20) | 5, 131072, 70000]
+    files = [gcz.gen_synthetic(300 + i, s, 8 << 20, tuple(rng.dirichlet([1, 1, 1]))) for i, s in enumerate(sizes)]
+    files[4] = _build({"kind": "zipf", "n": 65536, "seed": 9})
+    res = ctx.zstd_compress_files_gpu(files, 1)
+    assert len(res) == len(files)
+    for f, frames in zip(files, res):
+        blob, fs = ctx.zstd_compress_frames_gpu(f, 1)
+        assert frames == _split(blob, fs)
+        for b in (0, len(frames) - 1):
+            if frames:
+                win = f[b * W:(b + 1) * W]
+                assert codecs.zstd_decompress(frames[b], win.size) == win.tobytes()
+    # device form
+    foff, wins, slab = gcz.batch_layout([f.size for f in files])
+    h_slab = np.zeros(slab, np.uint8)
+    for o, f in zip(foff, files):
+        h_slab[int(o):int(o) + f.size] = f
+    d_slab = torch.from_numpy(h_slab).cuda()
+    d_wins = torch.from_numpy(wins.view(np.uint8)).cuda()
+    cap = sum(int(gcz.L.gcz_zstd_max_sequences(f.size)) for f in files)
+    d_seqs = torch.empty((max(cap, 1), 4), dtype=torch.int32, device="cuda")
+    d_off = torch.empty(wins.size + 1, dtype=torch.int64, device="cuda")
+    ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16, d_seqs.data_ptr(), cap,
+                                     d_off.data_ptr(), 0)
+    fb = sum(int(gcz.L.gcz_zstd_frames_bound(f.size)) for f in files)
+    d_out = torch.empty(fb, dtype=torch.uint8, device="cuda")
+    d_foff = torch.empty(wins.size + 1, dtype=torch.int64, device="cuda")
+    ctx.zstd_encode_frames_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, d_seqs.data_ptr(),
+                                        d_off.data_ptr(), d_out.data_ptr(), fb, d_foff.data_ptr(), 0)
+    ctx.sync(0)
+    foffs = d_foff.cpu().numpy().astype(np.uint64)
+    blob = d_out[:int(foffs[-1])].cpu().numpy()
+    assert _split(blob, np.diff(foffs)) == [fr for frames in res for fr in frames]
