@@ -75,6 +75,28 @@ def compress_zstd(data, level=1, device_id=0, threads=0):
     return write_container_frames(MAGIC_ZSTD, buf.size, WINDOW, sizes, blob)
 
 
+def compress_zstd_gpu(data, level=1, device_id=0):
+    """NVZS with frames built on the GPU (gcz_zstd_compress_frames_gpu): the
+    same container, decodable by the same reader and stock libzstd."""
+    from . import context
+
+    buf = np.frombuffer(memoryview(data).cast("B"), dtype=np.uint8)
+    if buf.size == 0:
+        return write_container(MAGIC_ZSTD, 0, WINDOW, [])
+    blob, sizes = context(device_id).zstd_compress_frames_gpu(buf, level)
+    return write_container_frames(MAGIC_ZSTD, buf.size, WINDOW, sizes, blob)
+
+
+def compress_zstd_files(files, level=1, device_id=0):
+    """One NVZS container per file for a whole batch, with one launch of each
+    GPU kernel for all of them (gcz_zstd_compress_files_gpu)."""
+    from . import context
+
+    bufs = [np.frombuffer(memoryview(f).cast("B"), dtype=np.uint8) for f in files]
+    frames = context(device_id).zstd_compress_files_gpu(bufs, level)
+    return [write_container(MAGIC_ZSTD, b.size, WINDOW, fr) for b, fr in zip(bufs, frames)]
+
+
 def compress_lzma2(data, device_id=0, workers=None):
     """NVLZ with one raw LZMA2 stream per 64 KiB window (the LZMA2 L1+ path):
     the GPU decides per window whether liblzma preset 9 runs at all, a pool of

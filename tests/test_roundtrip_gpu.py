@@ -136,3 +136,14 @@ def test_native_frames_empty_and_capacity(ctx):
                                         fs.ctypes.data, ctypes.byref(used))
     assert rc == -4 and used.value == 0  # GCZ_ECAPACITY
     assert b"too small" in gcz.L.gcz_last_error(ctx.handle)
+
+
+def test_nvzs_gpu_frames_and_file_batches_round_trip(ctx):
+    import gcz
+    from gcz import formats
+
+    data = gcz.gen_synthetic(14, 3 * 65536 + 11, 8 << 20)
+    assert formats.decompress(formats.compress_zstd_gpu(data.tobytes())) == data.tobytes()
+    files = [gcz.gen_synthetic(15 + i, s, 8 << 20).tobytes() for i, s in enumerate([0, 5, 70000, 200000])]
+    blobs = formats.compress_zstd_files(files)
+    assert [formats.decompress(b) for b in blobs] == files
