@@ -1092,8 +1092,10 @@ double now_ms() {
 }
 
 // Worst-case device bytes per input byte of one batch: slab 1, candidates 2,
-// Zstd packed 2.67, speculative lists 3.25, ZSTD_Sequence output 5.33.
-constexpr double kDeviceBytesPerInputByte = 14.5;
+// Zstd packed 2.67, speculative lists 3.25, ZSTD_Sequence output 5.33, and
+// for frames requests the frames 1.02, frame slots 1.02, offset codes 1.33
+// and plans 0.03.
+constexpr double kDeviceBytesPerInputByte = 18.0;
 
 struct ServerReq {
     uint64_t id = 0;
@@ -1184,6 +1186,25 @@ int server_launch(gcz_server *sv, int k) {
                                   sl.st, dw, nb)) != GCZ_OK)
             return r;
         GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
+    } else if (b.kind == GCZ_REQ_ZSTD_FRAMES) {
+        // sequences, then the GPU entropy stage; only the frame offsets come back now
+        size_t cap = 0, fbound = 0;
+        for (ServerReq *q : b.reqs) {
+            cap += gcz_zstd_max_sequences(q->n);
+            fbound += gcz_zstd_frames_bound(q->n);
+        }
+        if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.frames, std::max<size_t>(fbound, 1))) != GCZ_OK) return r;
+        if ((r = ensure_dev(c, sl.foff, (nb + 1) * 8)) != GCZ_OK) return r;
+        if ((r = ensure_host(c, sl.h_off, (nb + 1) * 8)) != GCZ_OK) return r;
+        uint64_t *d_off = static_cast<uint64_t *>(sl.offsets.p);
+        if ((r = zstd_device_core(c, sl.sc, slab_p, slab, b.depth, sl.seqs.p, cap, d_off, sl.st, dw, nb)) != GCZ_OK)
+            return r;
+        if ((r = zenc_core(c, sl.sc, slab_p, slab, sl.seqs.p, d_off, static_cast<uint8_t *>(sl.frames.p), fbound,
+                           static_cast<uint64_t *>(sl.foff.p), sl.st, dw, nb)) != GCZ_OK)
+            return r;
+        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.foff.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
     } else {
         if ((r = ensure_dev(c, sl.lz_packed, slab * 4 + 64)) != GCZ_OK) return r;
         if ((r = ensure_dev(c, sl.lz_has, nb + 16)) != GCZ_OK) return r;
@@ -1242,6 +1263,22 @@ void server_finish(gcz_server *sv, int k) {
                     r = GCZ_ECUDA;
             }
             if (cudaStreamSynchronize(sl.st) != cudaSuccess) r = GCZ_ECUDA;
+        } else if (r == GCZ_OK && b.kind == GCZ_REQ_ZSTD_FRAMES) {
+            const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);  // frame byte offsets
+            for (ServerReq *q : b.reqs) {
+                const uint64_t a = ho[q->w0], e = ho[q->w0 + q->nw];
+                uint64_t *ob = static_cast<uint64_t *>(q->out_b);
+                if (ob)
+                    for (uint32_t i = 0; i < q->nw; i++) ob[i] = ho[q->w0 + i + 1] - ho[q->w0 + i];
+                if (e - a > q->cap_a) {
+                    q->status = GCZ_ECAPACITY;
+                    continue;
+                }
+                if (e > a && cudaMemcpyAsync(q->out_a, static_cast<uint8_t *>(sl.frames.p) + a, e - a,
+                                             cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
+                    r = GCZ_ECUDA;
+            }
+            if (cudaStreamSynchronize(sl.st) != cudaSuccess) r = GCZ_ECUDA;
         }
         uint32_t h = 0;
         if (cudaMemcpy(&h, c->d_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) r = GCZ_ECUDA;
@@ -1278,7 +1315,7 @@ void server_loop(gcz_server *sv) {
             for (auto it = sv->pending.begin(); it != sv->pending.end();) {
                 ServerReq *q = *it;
                 const bool same = b.reqs.empty() ||
-                                  (q->kind == b.kind && (q->kind != 0 || (q->depth > 1) == (b.depth > 1)));
+                                  (q->kind == b.kind && (q->kind == GCZ_REQ_LZMA2 || (q->depth > 1) == (b.depth > 1)));
                 if (same && (b.reqs.empty() || (bytes + q->n <= sv->max_batch_bytes &&
                                                 b.reqs.size() < sv->max_batch_requests))) {
                     if (b.reqs.empty()) {
@@ -1353,8 +1390,9 @@ extern "C" void gcz_server_destroy(gcz_server *sv) {
         DeviceGuard g(sv->c->device);
         for (int j = 0; j < 2; j++) {
             Slot &sl = sv->slots[j];
-            for (DevBuf *b : {&sl.sc.packed, &sl.sc.counts, &sl.sc.cand, &sl.sc.seg, &sl.in, &sl.offsets, &sl.seqs,
-                              &sl.lz_packed, &sl.lz_has, &sv->wins[j]})
+            for (DevBuf *b : {&sl.sc.packed, &sl.sc.counts, &sl.sc.cand, &sl.sc.seg, &sl.sc.zslots, &sl.sc.zovs,
+                              &sl.sc.zaux, &sl.sc.zplan, &sl.in, &sl.offsets, &sl.seqs, &sl.lz_packed, &sl.lz_has,
+                              &sl.frames, &sl.foff, &sv->wins[j]})
                 if (b->p) cudaFree(b->p);
             if (sl.h_off.p) cudaFreeHost(sl.h_off.p);
             if (sl.ev) cudaEventDestroy(sl.ev);
@@ -1369,8 +1407,10 @@ extern "C" uint64_t gcz_server_max_batch_bytes(const gcz_server *sv) { return sv
 
 extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth, const uint8_t *src, size_t n,
                                  void *out_a, size_t cap_a, void *out_b, uint64_t *id) {
-    if (!sv || !id || (kind != GCZ_REQ_ZSTD && kind != GCZ_REQ_LZMA2) || (n && !src)) return GCZ_EINVAL;
+    if (!sv || !id || (kind != GCZ_REQ_ZSTD && kind != GCZ_REQ_LZMA2 && kind != GCZ_REQ_ZSTD_FRAMES) || (n && !src))
+        return GCZ_EINVAL;
     if (kind == GCZ_REQ_ZSTD && (!out_b || (n && !out_a))) return GCZ_EINVAL;
+    if (kind == GCZ_REQ_ZSTD_FRAMES && n && (!out_a || !out_b)) return GCZ_EINVAL;
     if (n > sv->max_batch_bytes) return GCZ_ETOOLARGE;
     ServerReq *q = new ServerReq();
     q->kind = kind;

@@ -6,7 +6,7 @@ import numpy as np
 
 from . import L, GczError, num_windows, _u8
 
-ZSTD, LZMA2 = 0, 1
+ZSTD, LZMA2, ZSTD_FRAMES = 0, 1, 2
 
 
 class Request:
@@ -15,7 +15,8 @@ class Request:
     out_a / out_b may be supplied (e.g. pinned, reused buffers): Zstd needs
     out_a u32[cap, 4] and out_b u64[windows+1]; LZMA2 takes out_a u32[n] or
     None (only the per-window has-match bytes, what the LZMA2 consumer reads)
-    and out_b u8[windows]."""
+    and out_b u8[windows]; ZSTD_FRAMES (frames built on the GPU) needs out_a
+    u8[cap] and out_b u64[windows] (frame sizes)."""
 
     def __init__(self, kind, data, depth, out_a=None, out_b=None, cap=None, packed=True):
         self.kind = kind
@@ -27,6 +28,10 @@ class Request:
             self.cap = int(L.gcz_zstd_max_sequences(n)) if cap is None else int(cap)
             self.out_a = np.empty((max(self.cap, 1), 4), np.uint32) if out_a is None else out_a
             self.out_b = np.zeros(nb + 1, np.uint64) if out_b is None else out_b
+        elif kind == ZSTD_FRAMES:
+            self.cap = int(L.gcz_zstd_frames_bound(n)) if cap is None else int(cap)
+            self.out_a = np.empty(max(self.cap, 1), np.uint8) if out_a is None else out_a
+            self.out_b = np.zeros(max(nb, 1), np.uint64) if out_b is None else out_b
         else:
             self.cap = n
             self.out_a = (np.empty(max(n, 1), np.uint32) if out_a is None else out_a) if packed else None
@@ -38,6 +43,12 @@ class Request:
         nb = num_windows(self.data.size)
         if self.kind == ZSTD:
             return self.out_a[:int(self.out_b[nb])], self.out_b[:nb + 1]
+        if self.kind == ZSTD_FRAMES:  # the frames, one per window
+            frames, pos = [], 0
+            for s in self.out_b[:nb].tolist():
+                frames.append(self.out_a[pos:pos + s].tobytes())
+                pos += s
+            return frames
         return (self.out_a[:self.data.size] if self.out_a is not None else None), self.out_b[:nb]
 
 
@@ -58,7 +69,7 @@ class Server:
         return int(L.gcz_server_max_batch_bytes(self._h))
 
     def submit(self, kind, data, depth=None, **outputs):
-        depth = (16 if kind == ZSTD else 32) if depth is None else depth
+        depth = (32 if kind == LZMA2 else 16) if depth is None else depth
         r = Request(kind, data, depth, **outputs)
         rid = ctypes.c_uint64()
         rc = L.gcz_server_submit(self._h, kind, depth, r.data.ctypes.data if r.data.size else None, r.data.size,

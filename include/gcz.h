@@ -229,13 +229,13 @@ int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const si
 /* A request loop over one context: requests of mixed kind and size are
  * submitted at any time and admitted into the next batch while its input stays
  * within max_batch_bytes (derived from hbm_budget: two batches are in flight,
- * each needing at most ~14.5 device bytes per input byte).  One worker thread
+ * each needing at most ~18 device bytes per input byte).  One worker thread
  * launches a batch on one stream while it completes the previous batch on the
  * other, so requests that arrive while a batch runs join the next one.  Every
  * request gets exactly the result it would get alone (windows are independent).
  * src and the output buffers must stay valid until gcz_server_wait returns. */
 typedef struct gcz_server gcz_server;
-enum { GCZ_REQ_ZSTD = 0, GCZ_REQ_LZMA2 = 1 };
+enum { GCZ_REQ_ZSTD = 0, GCZ_REQ_LZMA2 = 1, GCZ_REQ_ZSTD_FRAMES = 2 };
 
 int gcz_server_create(gcz_ctx *ctx, uint64_t hbm_budget, uint64_t max_batch_bytes, uint32_t max_batch_requests,
                       gcz_server **out);
@@ -243,7 +243,10 @@ void gcz_server_destroy(gcz_server *server);  /* finishes every submitted reques
 uint64_t gcz_server_max_batch_bytes(const gcz_server *server);
 /* GCZ_REQ_ZSTD: out_a = gcz_zstd_sequence[cap_a], out_b = uint64_t[num_windows+1] offsets.
  * GCZ_REQ_LZMA2: out_a = uint32_t[n] packed (or NULL), out_b = uint8_t[num_windows] has-match bytes
- * (or NULL); search_depth as for the direct calls.  GCZ_ETOOLARGE if n > max batch bytes. */
+ * (or NULL).  GCZ_REQ_ZSTD_FRAMES: the GPU frames of gcz_zstd_compress_frames_gpu -- out_a =
+ * uint8_t[cap_a] frames back to back (gcz_zstd_frames_bound(n) always suffices), out_b =
+ * uint64_t[num_windows] frame sizes.  search_depth as for the direct calls.  GCZ_ETOOLARGE if
+ * n > max batch bytes.  The HBM budget allows ~18 device bytes per input byte of a batch. */
 int gcz_server_submit(gcz_server *server, int kind, uint32_t search_depth, const uint8_t *src, size_t n, void *out_a,
                       size_t cap_a, void *out_b, uint64_t *request_id);
 /* Blocks until the request is done (or timeout_s passes: GCZ_EDEVICE) and returns its

@@ -79,3 +79,38 @@ def test_caller_buffers_and_has_only_lzma2(ctx):
         assert p is None
         np.testing.assert_array_equal(has, ctx.lzma2_match_find(data, 32)[1])
     srv.close()
+
+
+def test_frames_requests_in_a_mixed_stream(ctx):
+    """GCZ_REQ_ZSTD_FRAMES requests batched with the others: each gets exactly
+    the frames gcz_zstd_compress_frames_gpu gives for its bytes."""
+    import gcz
+    from gcz import serving, codecs
+
+    rng = np.random.default_rng(21)
+    sizes = [1, 300, 65536, 65537, 2 << 20, 100000, 0]
+    datas = [gcz.gen_synthetic(700 + i, s, 8 << 20, tuple(rng.dirichlet([1, 1, 1]))) for i, s in enumerate(sizes)]
+    srv = serving.Server(ctx, hbm_budget=4 * 10**9, max_batch_bytes=8 << 20)
+    reqs = []
+    for i, d in enumerate(datas):
+        reqs.append((serving.ZSTD_FRAMES, d, srv.submit(serving.ZSTD_FRAMES, d, 16)))
+        if i % 2 == 0:
+            reqs.append((serving.ZSTD, d, srv.submit(serving.ZSTD, d, 16)))
+    for kind, d, r in reqs:
+        res = srv.wait(r)
+        if kind == serving.ZSTD_FRAMES:
+            blob, fs = ctx.zstd_compress_frames_gpu(d, 1)
+            want, pos = [], 0
+            for s in fs.tolist():
+                want.append(blob[pos:pos + s].tobytes())
+                pos += s
+            assert res == want
+            if res:
+                assert codecs.zstd_decompress(res[0], min(d.size, 65536)) == d[:65536].tobytes()
+        else:
+            s, o = ctx.zstd_match_find(d, 16)
+            np.testing.assert_array_equal(res[1], o)
+            np.testing.assert_array_equal(res[0], s)
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] == len(reqs) and st["status"] == 0
