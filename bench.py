@@ -812,6 +812,9 @@ def run_frames(args):
 
 def main():
     args = parse()
+    single = args.workload in ("serving", "uneven", "frames")
+    if args.impl != "reference" and single and int(os.environ.get("RANK", "0")) != 0:
+        return  # one-GPU workloads: rank 0 runs and prints, the other ranks have no work
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "lzma2":
