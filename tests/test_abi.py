@@ -79,3 +79,16 @@ def test_null_context_is_an_error_not_a_crash():
     assert gcz.L.gcz_zstd_match_find(None, None, 0, 16, None, 0, None) == gcz._lib.GCZ_EINVAL
     assert gcz.L.gcz_lzma2_match_find(None, None, 0, 32, None, None) == gcz._lib.GCZ_EINVAL
     assert gcz.L.gcz_last_error(None) == b"null context"
+
+
+def test_c_example_compiles_against_the_header(tmp_path):
+    """The C host example builds with gcc against include/gcz.h and libgcz.so
+    (no GPU needed to compile and link)."""
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "gpu-compressor_b200", "gcz")
+    subprocess.run(["gcc", "-O2", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "gpu-compressor_b200", "examples", "gcz_compress.c"),
+                    "-L", libdir, "-lgcz", f"-Wl,-rpath,{libdir}", "-o", str(tmp_path / "gcz_compress")], check=True)

@@ -147,3 +147,27 @@ def test_nvzs_gpu_frames_and_file_batches_round_trip(ctx):
     files = [gcz.gen_synthetic(15 + i, s, 8 << 20).tobytes() for i, s in enumerate([0, 5, 70000, 200000])]
     blobs = formats.compress_zstd_files(files)
     assert [formats.decompress(b) for b in blobs] == files
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gpu_coder", [False, True])
+def test_c_example_writes_decodable_nvzs(ctx, tmp_path, gpu_coder):
+    """gpu-compressor_b200/examples/gcz_compress.c, built with gcc against the C
+    ABI only, writes an NVZS container that decodes to the input."""
+    import os
+    import subprocess
+    import gcz
+    from gcz import formats
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "gpu-compressor_b200", "gcz")
+    exe = tmp_path / "gcz_compress"
+    subprocess.run(["gcc", "-O2", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "gpu-compressor_b200", "examples", "gcz_compress.c"),
+                    "-L", libdir, "-lgcz", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    data = gcz.gen_synthetic(31, 5 * 65536 + 123, 8 << 20)
+    src, dst = tmp_path / "in.bin", tmp_path / "out.nvzs"
+    src.write_bytes(data.tobytes())
+    args = [str(exe), "-l", "2"] + (["-g"] if gpu_coder else []) + [str(src), str(dst)]
+    subprocess.run(args, check=True, capture_output=True)
+    assert formats.decompress(dst.read_bytes()) == data.tobytes()
