@@ -256,8 +256,6 @@ int gcz_server_wait(gcz_server *server, uint64_t request_id, double timeout_s, d
 int gcz_server_stats(gcz_server *server, uint64_t *completed, uint64_t *bytes, uint64_t *batches, double *p50_ms,
                      double *p99_ms);
 
-/* ---------------------------------------------------------------- timing */
-
 /* ---------------------------------------------------------------- frames */
 
 /* Zstd L1/L2 frames of a host buffer: compress_chunk_zstd_custom
@@ -316,6 +314,8 @@ int gcz_zstd_compress_files_gpu(gcz_ctx *ctx, const uint8_t *const *srcs, const 
                                 uint32_t level, uint8_t *out, size_t out_capacity, uint64_t *frame_sizes,
                                 size_t *out_size);
 
+/* ---------------------------------------------------------------- self-test, timing */
+
 /* Self-test of the error path (no counterpart in the reference): one CTA waits
  * on an mbarrier that nothing completes, with the same kind of bounded wait
  * the kernels use around their bulk copies; the wait runs out after
@@ -326,8 +326,9 @@ int gcz_selftest_wait_timeout(gcz_ctx *ctx, uint32_t max_iterations);
 /* Between gcz_profile_start and gcz_profile_stop every match-find step this
  * context launches is bracketed by CUDA events on its own launch stream.
  * gcz_profile_stop synchronises those events and returns the summed device
- * time of the match-find kernels, their launch count, and the count of all
- * kernels the library launched in that interval (match-find + compaction). */
+ * time of the match-find steps, their count, and the count of all kernels
+ * the library launched in that interval (match finding, compaction and the
+ * entropy stage). */
 int gcz_profile_start(gcz_ctx *ctx);
 int gcz_profile_stop(gcz_ctx *ctx, double *match_kernel_ms, uint64_t *match_kernel_launches,
                      uint64_t *all_kernel_launches);
