@@ -14,11 +14,11 @@
 // reads it back; when every lane reads back its own position no two lanes of
 // the step share a bucket, the values read are the candidates and the table
 // is up to date.  Otherwise (equal hashes inside a step) the table is restored
-// and __match_any_sync groups the lanes: the in-step predecessor is the next
-// lower lane of the group and the highest lane writes the bucket.  (On this
-// GPU __match_any_sync costs hundreds of cycles, so it is kept off the common
-// path.)  Only the table lives in shared memory (32 KiB), so seven windows are
-// swept per SM; the input streams through coalesced 128-byte loads.
+// from that step on, and in each step with equal hashes __match_any_sync
+// groups the lanes: the in-step predecessor is the next lower lane of the
+// group and the highest lane writes the bucket.  Only the table lives in
+// shared memory (32 KiB), so seven windows are swept per SM; the input streams
+// through coalesced 128-byte loads.
 #include "gcz_common.cuh"
 #include "gcz_kernels.h"
 
@@ -88,21 +88,29 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
                 if (v[j] && T[h[j]] != static_cast<uint16_t>(q)) dup |= 1u << j;
             }
             uint32_t g[4] = {1u << lane, 1u << lane, 1u << lane, 1u << lane};
-            if (__any_sync(kFull, dup != 0)) {
-                // Rare: some step has equal hashes in two lanes.  Put the table
-                // back as it was before the block (latest steps first, so each
-                // bucket ends with the value its earliest step read) and redo
-                // the block with exact groups.
+            const uint32_t dsteps = __reduce_or_sync(kFull, dup);  // steps with equal hashes in two lanes
+            if (dsteps) {
+                // One block in two on compressible data.  Steps before the
+                // first such step j0 wrote each bucket once and are exact.  Put
+                // the table back as it was before j0 (latest steps first, so
+                // each bucket ends with the value its earliest step from j0 on
+                // read) and redo from j0, grouping the lanes of the steps that
+                // share buckets.  Which lanes share a bucket depends only on
+                // the hashes, so the other steps need no groups.
+                const uint32_t j0 = static_cast<uint32_t>(__ffs(dsteps)) - 1u;
                 __syncwarp();
 #pragma unroll
                 for (int j = 3; j >= 0; --j) {
-                    if (v[j]) T[h[j]] = static_cast<uint16_t>(tv[j]);
-                    __syncwarp();
+                    if (static_cast<uint32_t>(j) >= j0) {
+                        if (v[j]) T[h[j]] = static_cast<uint16_t>(tv[j]);
+                        __syncwarp();
+                    }
                 }
 #pragma unroll
                 for (uint32_t j = 0; j < 4; ++j) {
+                    if (j < j0) continue;
                     const uint32_t q = blk * 128u + j * 32u + lane;
-                    g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+                    if ((dsteps >> j) & 1u) g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
                     tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
                     __syncwarp();
                     if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
