@@ -235,6 +235,37 @@ def cpu_oracle_time(data, depth, threads):
     return dt, int(off[-1])
 
 
+def link_time(torch, dev, h_in, d_in, h_out, d_out, out_bytes, piece=64 << 20, reps=3):
+    """Seconds for the PCIe traffic of one end-to-end step with no kernels:
+    the input's H2D in `piece`-sized copies on one stream while `out_bytes` of
+    results go D2H in matching pieces on another (full duplex, as in the
+    pipeline).  Mean of `reps` runs after one warm-up, CUDA events."""
+    src, dst = h_in.view(torch.uint8).reshape(-1), d_in.view(torch.uint8).reshape(-1)
+    osrc, odst = d_out.view(torch.uint8).reshape(-1)[:out_bytes], h_out.view(torch.uint8).reshape(-1)[:out_bytes]
+    n = src.numel()
+    k = max((n + piece - 1) // piece, 1)
+    opiece = (out_bytes + k - 1) // k
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    times = []
+    for r in range(reps + 1):
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s_in)
+        s_out.wait_event(e0)
+        for i in range(k):
+            with torch.cuda.stream(s_in):
+                dst[i * piece:(i + 1) * piece].copy_(src[i * piece:(i + 1) * piece], non_blocking=True)
+            if i * opiece < out_bytes:
+                with torch.cuda.stream(s_out):
+                    odst[i * opiece:(i + 1) * opiece].copy_(osrc[i * opiece:(i + 1) * opiece], non_blocking=True)
+        s_in.wait_stream(s_out)
+        e1.record(s_in)
+        torch.cuda.synchronize(dev)
+        if r:
+            times.append(e0.elapsed_time(e1) / 1e3)
+    return sum(times) / len(times)
+
+
 def run_gcz(args):
     import torch
     import gcz
@@ -281,7 +312,7 @@ def run_gcz(args):
     value = world * n * args.steps / (ms_max / 1e3) / 1e9
 
     # ---- end-to-end through the host-buffer C-ABI call (pinned buffers)
-    e2e_value = None
+    e2e_value = link_value = None
     if args.e2e_steps > 0:
         h_in = torch.from_numpy(data).pin_memory()
         h_seqs = torch.empty((nseq + 1024, 4), dtype=torch.int32).pin_memory()
@@ -303,6 +334,8 @@ def run_gcz(args):
         e2e_max = max_over_ranks(dist, torch, e2e_s)
         e2e_value = round(world * n * args.e2e_steps / e2e_max / 1e9, 3)
         assert int(h_off[-1].item()) == nseq
+        link_s = max_over_ranks(dist, torch, link_time(torch, dev, h_in, d_in, h_seqs, d_seqs, 16 * nseq))
+        link_value = round(world * n / link_s / 1e9, 3)
 
     # ---- roofline of the match-find step (match kernel + offset scan + compaction)
     peak, peak_kind = peaks()
@@ -335,7 +368,12 @@ def run_gcz(args):
                        "algo": args.algo, "fallback_windows": ctx.query("fallback_windows"),
                        "l2": "input 1 GiB > 126 MB L2, no flush needed"},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n,
-                    "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1)},
+                    "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1),
+                    "link_bound": {"value": link_value, "unit": "GB/s",
+                                   "what": "plain pinned copies of the step's bytes, no kernels: the H2D of the "
+                                           "input in 64 MiB pieces with the sequence records' D2H on a second "
+                                           "stream"},
+                    "frac_of_link": round(e2e_value / link_value, 3) if e2e_value and link_value else None},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms_per_step": round(step_ms, 4),
