@@ -768,7 +768,7 @@ def run_frames(args):
     """Zstd L2 frames end to end: 1 GiB host input (seed 2) -> one Zstd frame
     per 64 KiB window.  `value`: everything on the GPU
     (gcz_zstd_compress_frames_gpu: copy-in, match finding, entropy stage,
-    copy-out of 64 MiB slices on two streams).  Beside it: the libzstd coder
+    copy-out of 32 MiB slices over four streams).  Beside it: the libzstd coder
     path (gcz_zstd_compress_frames: GPU sequences, ZSTD_compressSequences on
     all host cores) and, on a 64 MiB sample, the reference's schedule (GPU
     sequences, then one thread encoding window after window,
@@ -839,7 +839,7 @@ def run_frames(args):
         "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
         "ms_per_step": round(1e3 * sec, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
-        "config": {"workload": "zstd_l2_frames_1gib", "input_bytes": n, "windows": nb, "slice": "64 MiB",
+        "config": {"workload": "zstd_l2_frames_1gib", "input_bytes": n, "windows": nb, "slice": "32 MiB, 4 slots",
                    "entropy_stage": "GPU: Huffman/RLE/raw literals, predefined-FSE sequences, repeat codes",
                    "compressed_bytes": gpu_bytes, "ratio": round(gpu_bytes / n, 4)},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": gpu_bytes},

@@ -77,7 +77,8 @@ const char *gcz_version(void);
  * CTAs per SM (1-8); "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 1024 = 64 MiB; two slices are in flight; slices ramp up
  * from a quarter of it and back down at the end); "frames_slice_windows" =
- * the same for gcz_zstd_compress_frames_gpu (default 4096 = 256 MiB). */
+ * the same for gcz_zstd_compress_frames_gpu (default 512 = 32 MiB; four
+ * slots, three slices in flight). */
 int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
 /* Read a knob or a counter: "algo" (1: fused single-warp kernels, 2: candidate
  * sweep + second stage, the default), "fallback_windows" (Zstd windows whose
