@@ -217,8 +217,9 @@ class Context:
         return out[:used.value], sizes[:num_windows(n)]
 
     def zstd_compress_frames_gpu(self, data, level=1):
-        """One Zstd frame per 64 KiB window, encoded on the GPU (raw literals,
-        predefined FSE tables): (frames back to back, frame sizes u64[B])."""
+        """One Zstd frame per 64 KiB window, encoded on the GPU (raw, RLE or
+        Huffman literals; predefined FSE sequence tables): (frames back to back,
+        frame sizes u64[B])."""
         src = _u8(data)
         n = src.size
         out = np.empty(max(int(L.gcz_zstd_frames_bound(n)), 1), np.uint8)

@@ -104,6 +104,30 @@ def test_gpu_frames_large_decode_and_level2(ctx):
 
 
 @pytest.mark.gpu
+def test_gpu_frames_pipeline_slices_do_not_change_bytes():
+    """The host pipeline rotates its slices over four slots and finishes them
+    in order.  Whatever the slice size -- one window per slice (every slot
+    reused hundreds of times), odd sizes, or the whole input in one slice --
+    the frames and the size table are the same bytes."""
+    import gcz
+
+    n = 20 * (1 << 20) + 999
+    data = gcz.gen_synthetic(31, n, 8 << 20)
+    c = gcz.Context(0)
+    try:
+        c.set_option("frames_slice_windows", 1 << 20)  # one slice
+        blob, sizes = c.zstd_compress_frames_gpu(data, 1)
+        assert sizes.size == gcz.num_windows(n) and int(sizes.sum()) == blob.size
+        for fsw in (1, 7, 64, 512):
+            c.set_option("frames_slice_windows", fsw)
+            b2, s2 = c.zstd_compress_frames_gpu(data, 1)
+            assert np.array_equal(s2, sizes), fsw
+            assert np.array_equal(b2, blob), fsw
+    finally:
+        c.close()
+
+
+@pytest.mark.gpu
 def test_device_entropy_stage_on_oracle_sequences(ctx):
     import torch
     import gcz
