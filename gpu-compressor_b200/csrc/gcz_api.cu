@@ -65,7 +65,7 @@ struct gcz_ctx {
     std::string err;
     uint32_t *d_status = nullptr;
     Scratch sc;      // scratch of the _device entry points
-    Slot slots[4];   // host-buffer pipelines (the GPU frames pipeline uses all four, the others two)
+    Slot slots[4];   // host-buffer pipelines (Zstd sequences and GPU frames rotate over all four, LZMA2 two)
     uint32_t slice_windows = 1024;         // windows per pipeline slice (64 MiB)
     uint32_t frames_slice_windows = 512;   // ... of the GPU frames pipeline (32 MiB, four slots)
     int staged = 1;
@@ -549,9 +549,12 @@ int drain_slots(gcz_ctx *c) {
 }
 }  // namespace
 
-// Slices of slice_windows windows alternate between two slots (streams): the
-// H2D copy and kernels of slice k run while slice k-1's sequences are copied
-// back.
+// Slices of slice_windows windows rotate over the S = 4 slots (streams): the
+// H2D copy and kernels of slice k run while earlier slices' sequences are
+// copied back.  Slice k is queued before the host waits for slice k-(S-1) and
+// queues its copy-out, so the host's wait never holds back the next copy-in
+// (two slots, finishing slice k-1: 47.7 GB/s for 1 GiB; four: 48.8, against
+// 51.8 for the same copies with no kernels).
 extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
                                    gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets) {
     if (!c) return GCZ_EINVAL;
@@ -562,9 +565,10 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
     offsets[0] = 0;
     int r = GCZ_OK;
     uint64_t done = 0;  // sequences copied so far
+    constexpr size_t kS = sizeof(c->slots) / sizeof(c->slots[0]);
     size_t k = 0;
     for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
-        Slot &sl = c->slots[k & 1];
+        Slot &sl = c->slots[k % kS];  // slice k-S, its last user, was finished one iteration ago
         sb = next_slice(b0, nb, c->slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
@@ -583,11 +587,15 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
         GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
         GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
         sl.busy = true;
-        Slot &prev = c->slots[(k + 1) & 1];
-        if (prev.busy) r = zstd_finish_slot(c, prev, seqs, seq_capacity, offsets, done);
+        if (k >= kS - 1) {  // finish slice k-(S-1); slices finish in order, so records stay in order
+            Slot &old = c->slots[(k - (kS - 1)) % kS];
+            if (old.busy) r = zstd_finish_slot(c, old, seqs, seq_capacity, offsets, done);
+        }
     }
-    Slot &last = c->slots[(k + 1) & 1];
-    if (r == GCZ_OK && last.busy) r = zstd_finish_slot(c, last, seqs, seq_capacity, offsets, done);
+    for (size_t j = k >= kS - 1 ? k - (kS - 1) : 0; j < k && r == GCZ_OK; ++j) {
+        Slot &rest = c->slots[j % kS];
+        if (rest.busy) r = zstd_finish_slot(c, rest, seqs, seq_capacity, offsets, done);
+    }
     for (Slot &sl : c->slots) sl.busy = false;
     const int r2 = drain_slots(c);
     return r != GCZ_OK ? r : r2;
