@@ -65,7 +65,7 @@ struct gcz_ctx {
     std::string err;
     uint32_t *d_status = nullptr;
     Scratch sc;      // scratch of the _device entry points
-    Slot slots[4];   // host-buffer pipelines (Zstd sequences and GPU frames rotate over all four, LZMA2 two)
+    Slot slots[4];   // host-buffer pipelines: each rotates over all four, three slices in flight
     uint32_t slice_windows = 1024;         // windows per pipeline slice (64 MiB)
     uint32_t frames_slice_windows = 512;   // ... of the GPU frames pipeline (32 MiB, four slots)
     int staged = 1;
@@ -779,9 +779,10 @@ extern "C" int gcz_lzma2_match_find_device(gcz_ctx *c, const uint8_t *d_src, siz
 }
 
 namespace {
-// Host-side slices for the two LZMA2 host entry points, alternating between
-// the two pipeline slots; `consume` sees each slice's packed results on the
-// host once they have arrived.
+// Host-side slices for the two LZMA2 host entry points, rotating over the
+// S = 4 pipeline slots like the Zstd pipeline (slice k is queued before the
+// host finishes slice k-(S-1)); `consume` sees each slice's packed results on
+// the host once they have arrived, in slice order.
 template <class Consume>
 int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, uint32_t *packed_out,
                      uint8_t *has_out, bool copy_packed, Consume consume) {
@@ -793,9 +794,10 @@ int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, u
         consume(sl.off, sl.len, packed_out ? packed_out + sl.off : static_cast<const uint32_t *>(sl.h_packed.p));
         return GCZ_OK;
     };
+    constexpr size_t kS = sizeof(c->slots) / sizeof(c->slots[0]);
     size_t k = 0;
     for (size_t b0 = 0, sb = 0; b0 < nb && r == GCZ_OK; b0 += sb, ++k) {
-        Slot &sl = c->slots[k & 1];
+        Slot &sl = c->slots[k % kS];  // slice k-S, its last user, was finished one iteration ago
         sb = next_slice(b0, nb, c->slice_windows);
         sl.b0 = b0;
         sl.sb = sb;
@@ -820,11 +822,15 @@ int lzma_host_slices(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t depth, u
         if (has_out) GCZ_CUDA(c, cudaMemcpyAsync(has_out + b0, sl.lz_has.p, sb, cudaMemcpyDeviceToHost, sl.st));
         GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
         sl.busy = true;
-        Slot &prev = c->slots[(k + 1) & 1];
-        if (prev.busy) r = finish(prev);
+        if (k >= kS - 1) {  // finish slice k-(S-1), in slice order
+            Slot &old = c->slots[(k - (kS - 1)) % kS];
+            if (old.busy) r = finish(old);
+        }
     }
-    Slot &last = c->slots[(k + 1) & 1];
-    if (r == GCZ_OK && last.busy) r = finish(last);
+    for (size_t j = k >= kS - 1 ? k - (kS - 1) : 0; j < k && r == GCZ_OK; ++j) {
+        Slot &rest = c->slots[j % kS];
+        if (rest.busy) r = finish(rest);
+    }
     for (Slot &sl : c->slots) sl.busy = false;
     const int r2 = drain_slots(c);
     return r != GCZ_OK ? r : r2;

@@ -75,9 +75,9 @@ const char *gcz_version(void);
  * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
  * memory with bulk copies, 0 reads it through L1; "parse_ctas" = second-stage
  * CTAs per SM (1-8); "slice_windows" = windows per slice of the host-buffer
- * pipelines (default 1024 = 64 MiB; Zstd rotates four slots, three slices
- * in flight, LZMA2 two; slices ramp up from a quarter of it and back down at
- * the end); "frames_slice_windows" =
+ * pipelines (default 1024 = 64 MiB; four slots, three slices in flight;
+ * slices ramp up from a quarter of it and back down at the end);
+ * "frames_slice_windows" =
  * the same for gcz_zstd_compress_frames_gpu (default 512 = 32 MiB; four
  * slots, three slices in flight). */
 int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
