@@ -277,16 +277,18 @@ int gcz_zstd_compress_frames(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_
 /* Zstd frames built on the GPU (no reference counterpart: the reference's
  * GPU block encoder, zstd_compress.cu:756-1038, is unused and its output is
  * not decodable).  Each 64 KiB window becomes one frame with a single block:
- * raw literals and sequences FSE-coded with the format's predefined
- * distributions (RFC 8878), repeat offsets used where they apply, or a raw
- * block when that is smaller.  Every frame decodes with stock libzstd to its
- * window.  The frames differ from libzstd's (no Huffman literals, no tuned
- * tables), so the ratio is somewhat higher than gcz_zstd_compress_frames'.
+ * literals raw, RLE or Huffman-coded (whichever is smallest), sequences
+ * FSE-coded with the format's predefined distributions (RFC 8878), repeat
+ * offsets used where they apply, or a raw block when that is smaller.  Every
+ * frame decodes with stock libzstd to its window.  The frames differ from
+ * libzstd's (predefined sequence tables, no tuned ones), so the ratio is a
+ * little higher than gcz_zstd_compress_frames' (0.6845 against 0.6775 on the
+ * bench data).
  *
  * gcz_zstd_compress_frames_gpu: host bytes in, frames back to back in `out`
  * (out_capacity >= gcz_zstd_frames_bound(n) always suffices) with
  * frame_sizes[num_windows]; copy-in, match finding, encoding and copy-out of
- * 64 MiB slices overlap on two streams.
+ * 32 MiB slices overlap over four streams ("frames_slice_windows").
  * gcz_zstd_encode_frames_device: the entropy stage alone, on device memory,
  * from the output of gcz_zstd_match_find_device (records + per-window
  * offsets): frames back to back in d_out, byte offsets of the frames in
