@@ -1161,7 +1161,11 @@ struct gcz_server {
     DevBuf wins[2];
     std::vector<gcz_window> hwins[2];
     Batch batch[2];
+    // Latencies of the most recent kLatWindow completed requests (a ring once
+    // full), so that a long-running loop's memory and stats cost stay bounded.
+    static constexpr size_t kLatWindow = size_t(1) << 20;
     std::vector<double> lat_ms;
+    size_t lat_next = 0;
     uint64_t completed = 0, bytes_done = 0, batches = 0;
     int worker_error = GCZ_OK;
 };
@@ -1313,7 +1317,13 @@ void server_finish(gcz_server *sv, int k) {
     for (ServerReq *q : b.reqs) {
         if (q->status == 1) q->status = r;
         q->t_done = t;
-        sv->lat_ms.push_back(q->t_done - q->t_submit);
+        const double lat = q->t_done - q->t_submit;
+        if (sv->lat_ms.size() < gcz_server::kLatWindow) {
+            sv->lat_ms.push_back(lat);
+        } else {
+            sv->lat_ms[sv->lat_next] = lat;
+            sv->lat_next = (sv->lat_next + 1) % gcz_server::kLatWindow;
+        }
         sv->completed++;
         sv->bytes_done += q->n;
     }
@@ -1335,19 +1345,25 @@ void server_loop(gcz_server *sv) {
             if (sv->pending.empty() && sv->stop && !other.busy) break;
             // Admit pending requests of the first request's kind (and Zstd lazy
             // mode) while the batch stays within the byte and count limits.
+            // Bytes are counted as laid out in the slab, each request padded to
+            // whole 64 KiB windows: every device buffer of a batch then stays
+            // within the size of one max_batch_bytes batch, so a burst of small
+            // requests never regrows (cudaFree synchronises the device) and the
+            // HBM budget holds.
             uint64_t bytes = 0;
             for (auto it = sv->pending.begin(); it != sv->pending.end();) {
                 ServerReq *q = *it;
+                const uint64_t padded = nwin(q->n) * (uint64_t)kW;
                 const bool same = b.reqs.empty() ||
                                   (q->kind == b.kind && (q->kind == GCZ_REQ_LZMA2 || (q->depth > 1) == (b.depth > 1)));
-                if (same && (b.reqs.empty() || (bytes + q->n <= sv->max_batch_bytes &&
+                if (same && (b.reqs.empty() || (bytes + padded <= sv->max_batch_bytes &&
                                                 b.reqs.size() < sv->max_batch_requests))) {
                     if (b.reqs.empty()) {
                         b.kind = q->kind;
                         b.depth = q->depth;
                     }
                     q->t_admit = now_ms();
-                    bytes += q->n;
+                    bytes += padded;
                     b.reqs.push_back(q);
                     it = sv->pending.erase(it);
                 } else {
@@ -1462,11 +1478,18 @@ extern "C" int gcz_server_wait(gcz_server *sv, uint64_t id, double timeout_s, do
     auto it = sv->reqs.find(id);
     if (it == sv->reqs.end()) return GCZ_EINVAL;
     ServerReq *q = it->second;
-    const bool ok = sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return q->status != 1; });
+    // wait_for releases the lock: submits from other threads may rehash the
+    // map (so the id is looked up again, never the iterator kept), and another
+    // waiter on the same id may take and free the request first (so q is read
+    // only while its id is still present).
+    auto gone = [&] { return sv->reqs.find(id) == sv->reqs.end(); };
+    const bool ok =
+        sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return gone() || q->status != 1; });
+    if (gone()) return GCZ_EINVAL;
     if (!ok) return GCZ_EDEVICE;
     const int st = q->status;
     if (latency_ms) *latency_ms = q->t_done - q->t_submit;
-    sv->reqs.erase(it);
+    sv->reqs.erase(id);
     delete q;
     return st;
 }
@@ -1474,16 +1497,21 @@ extern "C" int gcz_server_wait(gcz_server *sv, uint64_t id, double timeout_s, do
 extern "C" int gcz_server_stats(gcz_server *sv, uint64_t *completed, uint64_t *bytes, uint64_t *batches,
                                 double *p50_ms, double *p99_ms) {
     if (!sv) return GCZ_EINVAL;
-    std::lock_guard<std::mutex> lk(sv->mu);
-    std::vector<double> v = sv->lat_ms;
+    std::vector<double> v;
+    int err;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);  // copy under the lock, sort outside it (the worker takes it too)
+        v = sv->lat_ms;
+        if (completed) *completed = sv->completed;
+        if (bytes) *bytes = sv->bytes_done;
+        if (batches) *batches = sv->batches;
+        err = sv->worker_error;
+    }
     std::sort(v.begin(), v.end());
     auto pct = [&](double p) { return v.empty() ? 0.0 : v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))]; };
-    if (completed) *completed = sv->completed;
-    if (bytes) *bytes = sv->bytes_done;
-    if (batches) *batches = sv->batches;
     if (p50_ms) *p50_ms = pct(0.50);
     if (p99_ms) *p99_ms = pct(0.99);
-    return sv->worker_error;
+    return err;
 }
 
 // =========================================================================== profiling

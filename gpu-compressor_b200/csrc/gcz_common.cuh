@@ -1,6 +1,7 @@
 // Device-side building blocks shared by the Zstd and LZMA2 match finders.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -72,18 +73,22 @@ struct GlobalWin {
     }
 };
 
+// One bit per device: the kernel's shared-memory limit is set there.  Atomic,
+// because contexts on different host threads launch concurrently.
+using SmemOnce = std::atomic<unsigned long long>;
+
 // Sets a kernel's dynamic shared-memory limit once per device (host side), so
 // that later launches -- including ones being captured into a CUDA graph --
-// make no attribute calls.
+// make no attribute calls.  (Devices 64 and up set it on every launch.)
 template <class Kernel>
-inline cudaError_t set_smem_once(Kernel k, uint32_t bytes, unsigned long long &done_mask) {
+inline cudaError_t set_smem_once(Kernel k, uint32_t bytes, SmemOnce &done_mask) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const unsigned long long bit = 1ull << (dev & 63);
-    if (done_mask & bit) return cudaSuccess;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (bit && (done_mask.load(std::memory_order_acquire) & bit)) return cudaSuccess;
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-    if (e == cudaSuccess) done_mask |= bit;
+    if (e == cudaSuccess && bit) done_mask.fetch_or(bit, std::memory_order_acq_rel);
     return e;
 }
 

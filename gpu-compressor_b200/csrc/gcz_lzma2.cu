@@ -375,11 +375,11 @@ cudaError_t launch_lzma_match(const LzmaLaunch &l, cudaStream_t st) {
     const uint32_t smem = staged ? kSmemStaged : kSmemTable;
     cudaError_t e;
     if (staged) {
-        { static unsigned long long smem_set_1 = 0; e = set_smem_once(lzma_match_kernel<true>, smem, smem_set_1); }
+        { static SmemOnce smem_set_1{0}; e = set_smem_once(lzma_match_kernel<true>, smem, smem_set_1); }
         if (e != cudaSuccess) return e;
         lzma_match_kernel<true><<<grid, 32, smem, st>>>(a);
     } else {
-        { static unsigned long long smem_set_2 = 0; e = set_smem_once(lzma_match_kernel<false>, smem, smem_set_2); }
+        { static SmemOnce smem_set_2{0}; e = set_smem_once(lzma_match_kernel<false>, smem, smem_set_2); }
         if (e != cudaSuccess) return e;
         lzma_match_kernel<false><<<grid, 32, smem, st>>>(a);
     }
@@ -411,7 +411,7 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     a.status = l.status;
     a.wins = l.wins;
     const uint32_t smem = sizeof(L2Smem);
-    static unsigned long long smem_set_3 = 0;
+    static SmemOnce smem_set_3{0};
     cudaError_t e = set_smem_once(lzma_verify_kernel, smem, smem_set_3);
     if (e != cudaSuccess) return e;
     int grid = l.num_sms * 3;

@@ -139,7 +139,7 @@ cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, u
     if (num_windows == 0) return cudaSuccess;
     SweepArgs a{src, n, window, num_windows, cand, wins};
     const uint32_t smem = kSweepWarpsPerCta * kHashSize * sizeof(uint16_t);
-    static unsigned long long smem_set_1 = 0;
+    static SmemOnce smem_set_1{0};
     cudaError_t e = set_smem_once(cand_sweep_kernel, smem, smem_set_1);
     if (e != cudaSuccess) return e;
     uint32_t ctas = (num_windows + kSweepWarpsPerCta - 1) / kSweepWarpsPerCta;

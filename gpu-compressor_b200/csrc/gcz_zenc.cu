@@ -1209,7 +1209,7 @@ ZencArgs args_of(const ZencLaunch &l) {
     return a;
 }
 
-unsigned long long g_lit_smem_set = 0, g_seq_smem_set = 0, g_plan_smem_set = 0, g_write_smem_set = 0;
+SmemOnce g_lit_smem_set{0}, g_seq_smem_set{0}, g_plan_smem_set{0}, g_write_smem_set{0};
 
 }  // namespace
 

@@ -610,11 +610,11 @@ cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st) {
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
     cudaError_t e;
     if (l.ref_seqs) {
-        { static unsigned long long smem_set_1 = 0; e = set_smem_once(zstd_parse_kernel<true>, smem, smem_set_1); }
+        { static SmemOnce smem_set_1{0}; e = set_smem_once(zstd_parse_kernel<true>, smem, smem_set_1); }
         if (e != cudaSuccess) return e;
         zstd_parse_kernel<true><<<grid, kThreads, smem, st>>>(a);
     } else {
-        { static unsigned long long smem_set_2 = 0; e = set_smem_once(zstd_parse_kernel<false>, smem, smem_set_2); }
+        { static SmemOnce smem_set_2{0}; e = set_smem_once(zstd_parse_kernel<false>, smem, smem_set_2); }
         if (e != cudaSuccess) return e;
         zstd_parse_kernel<false><<<grid, kThreads, smem, st>>>(a);
     }

@@ -229,9 +229,12 @@ int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const si
 /* ---------------------------------------------------------------- serving */
 
 /* A request loop over one context: requests of mixed kind and size are
- * submitted at any time and admitted into the next batch while its input stays
- * within max_batch_bytes (derived from hbm_budget: two batches are in flight,
- * each needing at most ~18 device bytes per input byte).  One worker thread
+ * submitted at any time and admitted into the next batch while its input,
+ * each request counted in whole 64 KiB windows as it is laid out on the
+ * device, stays within max_batch_bytes (derived from hbm_budget: two batches
+ * are in flight, each needing at most ~18 device bytes per input byte).  So no
+ * batch needs more device memory than one max_batch_bytes batch, and once the
+ * buffers have grown to that (a first large batch), none regrows.  One worker thread
  * launches a batch on one stream while it completes the previous batch on the
  * other, so requests that arrive while a batch runs join the next one.  Every
  * request gets exactly the result it would get alone (windows are independent).
@@ -252,9 +255,11 @@ uint64_t gcz_server_max_batch_bytes(const gcz_server *server);
 int gcz_server_submit(gcz_server *server, int kind, uint32_t search_depth, const uint8_t *src, size_t n, void *out_a,
                       size_t cap_a, void *out_b, uint64_t *request_id);
 /* Blocks until the request is done (or timeout_s passes: GCZ_EDEVICE) and returns its
- * status; latency_ms = submit-to-completion time. */
+ * status; latency_ms = submit-to-completion time.  Each request is collected by
+ * one wait: GCZ_EINVAL for an unknown id or one already collected. */
 int gcz_server_wait(gcz_server *server, uint64_t request_id, double timeout_s, double *latency_ms);
-/* Completed requests, their input bytes, batches launched, latency percentiles (ms). */
+/* Completed requests, their input bytes, batches launched, and the p50/p99 of
+ * submit-to-completion latency (ms) over the most recent 2^20 completed requests. */
 int gcz_server_stats(gcz_server *server, uint64_t *completed, uint64_t *bytes, uint64_t *batches, double *p50_ms,
                      double *p99_ms);
 

@@ -46,6 +46,45 @@ def test_mixed_stream_equals_alone(ctx):
     assert st["p99_ms"] >= st["p50_ms"] > 0
 
 
+def test_wait_while_another_thread_submits(ctx):
+    """One thread submits while this one waits, so the request table grows and
+    rehashes under a blocked waiter; every request completes with its own
+    result, and waiting again on a request already collected is GCZ_EINVAL."""
+    import gcz
+    from gcz import serving
+
+    datas = [gcz.gen_synthetic(900 + i, 20000 + 37 * i, 8 << 20) for i in range(600)]
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=4 << 20)
+    reqs = []
+    cv = threading.Condition()
+
+    def submitter():
+        for d in datas:
+            r = srv.submit(serving.ZSTD, d, 16)
+            with cv:
+                reqs.append(r)
+                cv.notify()
+
+    t = threading.Thread(target=submitter)
+    t.start()
+    got = []
+    for i in range(len(datas)):
+        with cv:
+            cv.wait_for(lambda: len(reqs) > i)
+            r = reqs[i]
+        got.append(srv.wait(r))
+    t.join()
+    for i in (0, 299, 599):
+        s, o = ctx.zstd_match_find(datas[i], 16)
+        np.testing.assert_array_equal(got[i][1], o)
+        np.testing.assert_array_equal(got[i][0], s)
+    with pytest.raises(gcz.GczError) as e:
+        srv.wait(reqs[0])
+    assert e.value.code == gcz._lib.GCZ_EINVAL
+    assert srv.stats()["completed"] == len(datas)
+    srv.close()
+
+
 def test_oversized_request_is_rejected(ctx):
     import gcz
     from gcz import serving
