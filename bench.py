@@ -563,9 +563,12 @@ def run_serving(args):
             i += 1
 
     # Warm-up outside the timed region: two largest batches of each kind, so both
-    # slots of the loop hold their device buffers at full size.
+    # slots of the loop hold their device buffers at full size.  The loop flips
+    # slots on every batch, so the two of a kind go back to back (Z, Z, L, L);
+    # alternating kinds would leave each slot warm for one kind only, and the
+    # other kind's first batches there would allocate inside the timed region.
     wn = min(args.max_batch, pool_n)
-    for kind in (serving.ZSTD, serving.LZMA2, serving.ZSTD, serving.LZMA2):
+    for kind in (serving.ZSTD, serving.ZSTD, serving.LZMA2, serving.LZMA2):
         if kind == serving.ZSTD:
             cap = wn // 16 + 1024
             r = srv.submit(kind, pool_np[:wn], 16, out_a=ring[:cap * 16].view(np.uint32).reshape(cap, 4), cap=cap,

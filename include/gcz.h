@@ -238,7 +238,11 @@ int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const si
  * launches a batch on one stream while it completes the previous batch on the
  * other, so requests that arrive while a batch runs join the next one.  Every
  * request gets exactly the result it would get alone (windows are independent).
- * src and the output buffers must stay valid until gcz_server_wait returns. */
+ * src and the output buffers must stay valid until gcz_server_wait returns.
+ * The first batch of a kind on each of the two slots allocates that kind's
+ * device buffers (cudaMalloc; cudaFree before a regrowth waits for the
+ * device): two max-size requests of each kind, back to back, warm both slots
+ * before traffic whose latency matters. */
 typedef struct gcz_server gcz_server;
 enum { GCZ_REQ_ZSTD = 0, GCZ_REQ_LZMA2 = 1, GCZ_REQ_ZSTD_FRAMES = 2 };
 
