@@ -68,6 +68,26 @@ class Server:
     def max_batch_bytes(self):
         return int(L.gcz_server_max_batch_bytes(self._h))
 
+    def warm_up(self, kinds=(ZSTD, LZMA2)):
+        """Grow both slots' device buffers to a full batch of each kind before
+        latency-sensitive traffic: two max-size requests per kind, back to
+        back, because the worker alternates slots on every batch.  The device
+        buffers are sized from byte and window counts, not from the content, so
+        zero bytes do (with small host outputs: zero windows give one sequence,
+        or one tiny frame, each)."""
+        n = self.max_batch_bytes
+        nb = num_windows(n)
+        data = np.zeros(n, np.uint8)
+        for kind in kinds:
+            for _ in range(2):
+                if kind == ZSTD:
+                    r = self.submit(kind, data, out_a=np.empty((4 * nb, 4), np.uint32), cap=4 * nb)
+                elif kind == ZSTD_FRAMES:
+                    r = self.submit(kind, data, out_a=np.empty(64 * nb, np.uint8), cap=64 * nb)
+                else:
+                    r = self.submit(kind, data, packed=False)
+                self.wait(r)
+
     def submit(self, kind, data, depth=None, **outputs):
         depth = (32 if kind == LZMA2 else 16) if depth is None else depth
         r = Request(kind, data, depth, **outputs)

@@ -85,6 +85,23 @@ def test_wait_while_another_thread_submits(ctx):
     srv.close()
 
 
+def test_warm_up_then_serve(ctx):
+    """warm_up grows both slots for every kind (zero bytes, small host
+    outputs); requests served afterwards still get their own results."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=4 << 20)
+    srv.warm_up((serving.ZSTD, serving.LZMA2, serving.ZSTD_FRAMES))
+    assert srv.stats()["completed"] == 6
+    data = gcz.gen_synthetic(77, 3 << 20, 8 << 20)
+    seqs, off = srv.wait(srv.submit(serving.ZSTD, data, 16))
+    s, o = ctx.zstd_match_find(data, 16)
+    np.testing.assert_array_equal(off, o)
+    np.testing.assert_array_equal(seqs, s)
+    srv.close()
+
+
 def test_oversized_request_is_rejected(ctx):
     import gcz
     from gcz import serving
