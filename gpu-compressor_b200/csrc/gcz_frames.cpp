@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <type_traits>
@@ -156,7 +157,19 @@ extern "C" int gcz_zstd_compress_frames(gcz_ctx *c, const uint8_t *src, size_t n
     const uint32_t depth = gcz_zstd_search_depth_for_level(level);
     if (threads == 0) threads = std::max(1u, std::thread::hardware_concurrency());
 
-    std::vector<void *> cctx(threads, nullptr);
+    // 512-window (32 MiB) slices: small enough that filling and draining the
+    // pipeline costs little, large enough for one GPU call to amortise its launches.
+    constexpr size_t kSliceWindows = 512;
+    // Allocation failures before any coder thread runs are reported, not
+    // thrown through the C ABI.
+    std::vector<void *> cctx;
+    std::vector<uint8_t> stage;
+    try {
+        cctx.assign(threads, nullptr);
+        stage.resize(kSliceWindows * frame_bound(kW));
+    } catch (const std::bad_alloc &) {
+        return gcz_internal_fail(c, GCZ_ENOMEM, "host buffer allocation failed");
+    }
     auto free_all = [&] {
         for (void *p : cctx)
             if (p) z.freeCCtx(p);
@@ -169,13 +182,10 @@ extern "C" int gcz_zstd_compress_frames(gcz_ctx *c, const uint8_t *src, size_t n
         z.setParameter(p, kParam1001, 0);
     }
 
-    // 512-window (32 MiB) slices: small enough that filling and draining the
-    // pipeline costs little, large enough for one GPU call to amortise its launches.
     const size_t nb_all = gcz_num_windows(n);
-    const size_t slice_w = 512;
+    const size_t slice_w = kSliceWindows;
     const size_t nslices = (nb_all + slice_w - 1) / slice_w;
     SliceBufs bufs[2];
-    std::vector<uint8_t> stage(slice_w * frame_bound(kW));
     auto find = [&](size_t k, SliceBufs &sb) {
         const size_t off = k * slice_w * kW, len = std::min(n - off, slice_w * kW);
         const size_t cap = gcz_zstd_max_sequences(len);
@@ -205,8 +215,17 @@ extern "C" int gcz_zstd_compress_frames(gcz_ctx *c, const uint8_t *src, size_t n
         job.stage = stage.data();
         job.sizes = frame_sizes + k * slice_w;
         std::vector<std::thread> pool;
-        for (uint32_t t = 0; t < threads; ++t) pool.emplace_back([&, t] { encode_windows(z, cctx[t], job); });
+        uint32_t started = 0;
+        try {
+            pool.reserve(threads);
+            for (; started < threads; ++started)
+                pool.emplace_back([&, t = started] { encode_windows(z, cctx[t], job); });
+        } catch (const std::exception &) {
+            // Fewer threads than asked (a thread limit): windows are claimed one
+            // at a time by whoever is free, so the calling thread takes a share.
+        }
         if (k + 1 < nslices) find(k + 1, bufs[(k + 1) & 1]);  // GPU works on the next slice meanwhile
+        if (started < threads) encode_windows(z, cctx[started], job);
         for (std::thread &th : pool) th.join();
         if (job.failed.load()) {
             rc = gcz_internal_fail(c, GCZ_ECODEC, job.err.c_str());
