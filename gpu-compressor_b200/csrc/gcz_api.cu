@@ -7,6 +7,7 @@
 #include <cstring>
 #include <deque>
 #include <mutex>
+#include <new>
 #include <string>
 #include <thread>
 #include <unordered_map>
@@ -341,7 +342,8 @@ extern "C" int gcz_create(int device_id, gcz_ctx **out) {
         cudaGetLastError();
         return GCZ_EINVAL;
     }
-    gcz_ctx *c = new gcz_ctx();
+    gcz_ctx *c = new (std::nothrow) gcz_ctx();
+    if (!c) return GCZ_ENOMEM;
     c->device = device_id;
     DeviceGuard g(device_id);
     cudaDeviceProp prop;
@@ -1393,8 +1395,18 @@ extern "C" int gcz_server_create(gcz_ctx *c, uint64_t hbm_budget, uint64_t max_b
                                  uint32_t max_batch_requests, gcz_server **out) {
     if (!c || !out) return GCZ_EINVAL;
     *out = nullptr;
-    gcz_server *sv = new gcz_server();
+    gcz_server *sv = new (std::nothrow) gcz_server();
+    if (!sv) return fail(c, GCZ_ENOMEM, "server allocation failed");
     sv->c = c;
+    // Failure after this point: release the streams and events made so far.
+    auto release = [&] {
+        DeviceGuard g(c->device);
+        for (Slot &sl : sv->slots) {
+            if (sl.ev) cudaEventDestroy(sl.ev);
+            if (sl.st) cudaStreamDestroy(sl.st);
+        }
+        delete sv;
+    };
     uint64_t cap = (uint64_t)(hbm_budget / (2.0 * kDeviceBytesPerInputByte));
     if (max_batch_bytes == 0 || max_batch_bytes > cap) max_batch_bytes = cap;
     sv->max_batch_bytes = max_batch_bytes & ~uint64_t(kW - 1);
@@ -1409,11 +1421,16 @@ extern "C" int gcz_server_create(gcz_ctx *c, uint64_t hbm_budget, uint64_t max_b
             if (cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess ||
                 cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
                 cudaGetLastError();
-                delete sv;
+                release();
                 return GCZ_ECUDA;
             }
     }
-    sv->worker = std::thread(server_loop, sv);
+    try {
+        sv->worker = std::thread(server_loop, sv);
+    } catch (const std::exception &) {  // a thread limit: report it, never throw through the C ABI
+        release();
+        return fail(c, GCZ_ENOMEM, "could not start the request loop's worker thread");
+    }
     *out = sv;
     return GCZ_OK;
 }
@@ -1452,7 +1469,8 @@ extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth
     if (kind == GCZ_REQ_ZSTD && (!out_b || (n && !out_a))) return GCZ_EINVAL;
     if (kind == GCZ_REQ_ZSTD_FRAMES && n && (!out_a || !out_b)) return GCZ_EINVAL;
     if (n > sv->max_batch_bytes) return GCZ_ETOOLARGE;
-    ServerReq *q = new ServerReq();
+    ServerReq *q = new (std::nothrow) ServerReq();
+    if (!q) return GCZ_ENOMEM;
     q->kind = kind;
     q->depth = search_depth;
     q->src = src;
@@ -1464,8 +1482,14 @@ extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         q->id = sv->next_id++;
-        sv->reqs[q->id] = q;
-        sv->pending.push_back(q);
+        try {
+            sv->reqs[q->id] = q;
+            sv->pending.push_back(q);
+        } catch (const std::exception &) {  // out of host memory: not thrown through the C ABI
+            sv->reqs.erase(q->id);
+            delete q;
+            return GCZ_ENOMEM;
+        }
         *id = q->id;
     }
     sv->cv_work.notify_one();
