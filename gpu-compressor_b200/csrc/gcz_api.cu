@@ -1133,7 +1133,8 @@ struct ServerReq {
     size_t cap_a = 0;
     void *out_b = nullptr;
     double t_submit = 0, t_admit = 0, t_done = 0;
-    int status = 1;  // 1 = pending
+    int status = 1;  // 1 = pending; written under the server's mutex only (waiters read it there)
+    int fail = 0;    // the worker's own note of this request's failure, published as status on completion
     uint32_t w0 = 0, nw = 0;
     uint64_t slab_off = 0;
 };
@@ -1143,6 +1144,7 @@ struct Batch {
     int kind = 0;
     uint32_t depth = 0;
     uint32_t nb = 0;
+    int err = 0;  // status of the batch's launch (GCZ_OK or why it failed part-way)
     bool busy = false;
 };
 
@@ -1272,8 +1274,13 @@ void server_finish(gcz_server *sv, int k) {
     gcz_ctx *c = sv->c;
     Batch &b = sv->batch[k];
     Slot &sl = sv->slots[k];
-    int r = GCZ_OK;
-    {
+    int r = b.err;  // a launch that failed part-way completes its requests with its status
+    if (r != GCZ_OK) {
+        // Copies that the failed launch did queue end before the requests go back.
+        DeviceGuard g(c->device);
+        cudaStreamSynchronize(sl.st);
+        cudaGetLastError();
+    } else {
         DeviceGuard g(c->device);
         if (cudaEventSynchronize(sl.ev) != cudaSuccess) r = GCZ_ECUDA;
         if (r == GCZ_OK && b.kind == 0) {
@@ -1284,7 +1291,7 @@ void server_finish(gcz_server *sv, int k) {
                 if (ob)
                     for (uint32_t i = 0; i <= q->nw; i++) ob[i] = ho[q->w0 + i] - a;
                 if (e - a > q->cap_a) {
-                    q->status = GCZ_ECAPACITY;
+                    q->fail = GCZ_ECAPACITY;
                     continue;
                 }
                 if (e > a &&
@@ -1301,7 +1308,7 @@ void server_finish(gcz_server *sv, int k) {
                 if (ob)
                     for (uint32_t i = 0; i < q->nw; i++) ob[i] = ho[q->w0 + i + 1] - ho[q->w0 + i];
                 if (e - a > q->cap_a) {
-                    q->status = GCZ_ECAPACITY;
+                    q->fail = GCZ_ECAPACITY;
                     continue;
                 }
                 if (e > a && cudaMemcpyAsync(q->out_a, static_cast<uint8_t *>(sl.frames.p) + a, e - a,
@@ -1317,7 +1324,7 @@ void server_finish(gcz_server *sv, int k) {
     const double t = now_ms();
     std::lock_guard<std::mutex> lk(sv->mu);
     for (ServerReq *q : b.reqs) {
-        if (q->status == 1) q->status = r;
+        if (q->status == 1) q->status = q->fail != GCZ_OK ? q->fail : r;
         q->t_done = t;
         const double lat = q->t_done - q->t_submit;
         if (sv->lat_ms.size() < gcz_server::kLatWindow) {
@@ -1374,11 +1381,19 @@ void server_loop(gcz_server *sv) {
             }
         }
         if (!b.reqs.empty()) {
-            const int r = server_launch(sv, k);
+            // A failed launch is recorded on the batch; server_finish completes
+            // its requests.  Setting their status here would let a waiter free
+            // a request the batch still holds.
+            int r;
+            try {
+                r = server_launch(sv, k);
+            } catch (const std::exception &) {  // host memory: never let it end the worker thread
+                r = GCZ_ENOMEM;
+            }
+            b.err = r;
             b.busy = true;
             if (r != GCZ_OK) {
                 std::lock_guard<std::mutex> lk(sv->mu);
-                for (ServerReq *q : b.reqs) q->status = r;
                 sv->worker_error = r;
             }
         }

@@ -102,6 +102,28 @@ def test_warm_up_then_serve(ctx):
     srv.close()
 
 
+def test_short_output_fails_only_its_request(ctx):
+    """A Zstd request whose output room is too small completes with
+    GCZ_ECAPACITY; a request in the same batch gets its own result."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=8 << 20)
+    small = gcz.gen_synthetic(61, 1 << 20, 8 << 20)
+    good = gcz.gen_synthetic(62, 1 << 20, 8 << 20)
+    for _ in range(3):
+        r_small = srv.submit(serving.ZSTD, small, 16, out_a=np.empty((4, 4), np.uint32), cap=4)
+        r_good = srv.submit(serving.ZSTD, good, 16)
+        with pytest.raises(gcz.GczError) as e:
+            srv.wait(r_small)
+        assert e.value.code == gcz._lib.GCZ_ECAPACITY
+        seqs, off = srv.wait(r_good)
+        s, o = ctx.zstd_match_find(good, 16)
+        np.testing.assert_array_equal(off, o)
+        np.testing.assert_array_equal(seqs, s)
+    srv.close()
+
+
 def test_oversized_request_is_rejected(ctx):
     import gcz
     from gcz import serving
