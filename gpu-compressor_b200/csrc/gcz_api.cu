@@ -434,30 +434,6 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
     return fail(c, GCZ_EINVAL, "unknown option '%s'", key);
 }
 
-extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
-    if (!c || !key || !value) return GCZ_EINVAL;
-    std::lock_guard<std::mutex> lk(c->mu);
-    if (!strcmp(key, "algo")) {
-        *value = c->algo;
-        return GCZ_OK;
-    }
-    if (!strcmp(key, "fallback_windows")) {  // windows whose speculative parse fell back (since creation)
-        DeviceGuard g(c->device);
-        uint32_t h[2] = {0, 0};
-        GCZ_CUDA(c, cudaMemcpy(h, c->d_status, 8, cudaMemcpyDeviceToHost));
-        *value = (long)h[1];
-        return GCZ_OK;
-    }
-    return fail(c, GCZ_EINVAL, "unknown key '%s'", key);
-}
-
-extern "C" int gcz_sync(gcz_ctx *c, void *stream) {
-    if (!c) return GCZ_EINVAL;
-    std::lock_guard<std::mutex> lk(c->mu);
-    DeviceGuard g(c->device);
-    return read_status(c, pick_stream(c, stream));
-}
-
 namespace {
 // One CTA waits on an mbarrier that nothing will ever complete.  The wait is
 // bounded like every wait in the match finders; when it runs out the kernel
@@ -472,6 +448,40 @@ __global__ void selftest_wait_kernel(uint32_t *status, uint32_t max_iter) {
     if (threadIdx.x == 0 && !gcz::mbar_wait(&bar, 0u, max_iter)) atomicOr(status, gcz::kErrTmaTimeout);
 }
 }  // namespace
+
+extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
+    if (!c || !key || !value) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!strcmp(key, "algo")) {
+        *value = c->algo;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "fallback_windows")) {  // windows whose speculative parse fell back (since creation)
+        DeviceGuard g(c->device);
+        uint32_t h[2] = {0, 0};
+        GCZ_CUDA(c, cudaMemcpy(h, c->d_status, 8, cudaMemcpyDeviceToHost));
+        *value = (long)h[1];
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "binary_version") || !strcmp(key, "ptx_version")) {
+        // The architecture the loaded kernel image was compiled for, as the
+        // runtime reports it (major * 10 + minor: 100 for sm_100a).
+        DeviceGuard g(c->device);
+        cudaFuncAttributes fa{};
+        GCZ_CUDA(c, cudaFuncGetAttributes(&fa, selftest_wait_kernel));
+        *value = key[0] == 'b' ? (long)fa.binaryVersion : (long)fa.ptxVersion;
+        return GCZ_OK;
+    }
+    return fail(c, GCZ_EINVAL, "unknown key '%s'", key);
+}
+
+extern "C" int gcz_sync(gcz_ctx *c, void *stream) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    return read_status(c, pick_stream(c, stream));
+}
+
 
 extern "C" int gcz_selftest_wait_timeout(gcz_ctx *c, uint32_t max_iterations) {
     if (!c) return GCZ_EINVAL;

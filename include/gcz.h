@@ -83,7 +83,9 @@ const char *gcz_version(void);
 int gcz_set_option(gcz_ctx *ctx, const char *key, long value);
 /* Read a knob or a counter: "algo" (1: fused single-warp kernels, 2: candidate
  * sweep + second stage, the default), "fallback_windows" (Zstd windows whose
- * speculative parse fell back to the exact warp-wide parse, since creation). */
+ * speculative parse fell back to the exact warp-wide parse, since creation),
+ * "binary_version" / "ptx_version" (the architecture of the loaded kernel
+ * image as the CUDA runtime reports it, major*10+minor: 100 for sm_100a). */
 int gcz_query(gcz_ctx *ctx, const char *key, long *value);
 
 /* Synchronise `stream` (NULL = the context's stream) and report any error

@@ -18,7 +18,7 @@
  *
  * Parity is pinned against the reference kernels themselves: the fixtures in
  * tests/golden/ were produced by running the reference's own PTX (compiled from
- * its unmodified .cu sources) on a B200, and test_oracle_golden.py checks this
+ * its unmodified .cu sources) on a B200, and tests/test_oracle.py checks this
  * file against them.
  */
 #include <stdint.h>

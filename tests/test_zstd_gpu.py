@@ -165,3 +165,9 @@ def test_invalid_arguments(ctx):
         rc = gcz.L.gcz_zstd_match_find_ref_layout_device(ctx.handle, buf.data_ptr(), out.data_ptr(), None,
                                                          out.data_ptr(), None, w, 1, 100, 16, 100, None)
         assert rc == gcz._lib.GCZ_EINVAL
+
+
+def test_loaded_kernel_image_is_sm100(ctx):
+    """The kernels the runtime loaded from libgcz.so were compiled for sm_100a
+    (binaryVersion 100 from cudaFuncGetAttributes), not JIT-compiled from PTX."""
+    assert ctx.query("binary_version") == 100

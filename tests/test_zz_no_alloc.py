@@ -57,6 +57,38 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls():
     ctx.close()
 
 
+@pytest.mark.parametrize("depth", [1, 16], ids=["greedy", "lazy"])
+@pytest.mark.parametrize("n", [1, 7, 15, 65536, 65536 + 17], ids=["1B", "7B", "15B", "one-window", "window+17"])
+def test_noalloc_matches_allocating_entry_point_small_and_greedy(depth, n):
+    """Inputs shorter than one 16-byte bulk copy (read with plain loads),
+    exactly one window and one window plus a ragged tail, each with the greedy
+    parse (depth 1) and the lazy one (depth 16)."""
+    import torch
+    import gcz
+
+    torch.cuda.set_device(0)
+    ctx = gcz.Context(0)
+    st = _stream_handle(torch)
+    data = gcz.gen_synthetic(50 + n, n, 8 << 20)
+    d_in = torch.from_numpy(data).cuda()
+    B = gcz.num_windows(n)
+    cap = max(int(gcz.L.gcz_zstd_max_sequences(n)), 1)
+    want_seqs = torch.zeros((cap, 4), dtype=torch.int32, device="cuda")
+    want_off = torch.zeros(B + 1, dtype=torch.int64, device="cuda")
+    ctx.zstd_match_find_device(d_in.data_ptr(), n, depth, want_seqs.data_ptr(), cap, want_off.data_ptr(), st)
+    ctx.sync(st)
+    got_seqs = torch.full((cap, 4), -1, dtype=torch.int32, device="cuda")
+    got_off = torch.full((B + 1,), -1, dtype=torch.int64, device="cuda")
+    rc = gcz.L.gcz_zstd_match_find_device_noalloc(0, d_in.data_ptr(), n, depth, got_seqs.data_ptr(), cap,
+                                                  got_off.data_ptr(), st or None)
+    assert rc == gcz._lib.GCZ_OK
+    w_off = want_off.cpu().numpy()
+    np.testing.assert_array_equal(got_off.cpu().numpy(), w_off)
+    total = int(w_off[-1])
+    np.testing.assert_array_equal(got_seqs[:total].cpu().numpy(), want_seqs[:total].cpu().numpy())
+    ctx.close()
+
+
 def test_noalloc_rejects_oversized_input_and_bad_arguments():
     import torch
     import gcz
