@@ -33,7 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "gpu-compressor_b200"))
 sys.path.insert(0, ROOT)
 
-METRIC = "input GB/s per B200 (match-find, end-to-end)"
+METRIC = "input GB/s per B200 (match-find, end-to-end); p50/p99 latency; ratio, bit-exact"
 WORKLOAD = "zstd_l2_batched_1gib"
 N_BYTES = 1 << 30
 SEED = 2
@@ -50,16 +50,18 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3, help="0 skips the end-to-end leg")
     ap.add_argument("--bytes", type=int, default=N_BYTES, help="input bytes per GPU (profiling runs use less)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the other configs' keys (zstd_l1_16mib, ...)")
+    ap.add_argument("--no-heavy-configs", action="store_true", help="skip the uneven-batch and serving keys")
     ap.add_argument("--algo", type=int, default=2, help="1: fused single-warp kernels, 2: sweep + second stage")
     ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2", "serving", "uneven", "frames"],
                     help="zstd: Zstd L2 batched 1 GiB (the reported line); lzma2: LZMA2 L1 1 GiB, seed 3; "
                          "serving: open-loop request stream; uneven: many files in one launch")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second (Poisson)")
-    ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
-    ap.add_argument("--max-request", type=int, default=64 << 20, help="serving: largest request size")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    ap.add_argument("--max-request", type=int, default=256 << 20, help="serving: largest request size")
     ap.add_argument("--max-batch", type=int, default=256 << 20, help="serving: largest batch (bytes of input)")
     ap.add_argument("--files", type=int, default=4096, help="uneven: number of files")
-    ap.add_argument("--max-file", type=int, default=8 << 20, help="uneven: largest file size")
+    ap.add_argument("--max-file", type=int, default=64 << 20, help="uneven: largest file size")
     return ap.parse_args()
 
 
@@ -266,6 +268,139 @@ def link_time(torch, dev, h_in, d_in, h_out, d_out, out_bytes, piece=64 << 20, r
     return sum(times) / len(times)
 
 
+def time_steps(torch, stream, steps, fn, flush=None):
+    """Mean milliseconds per call of fn() with CUDA events on `stream`.  With no
+    `flush`, one event pair brackets all steps (inputs larger than L2).  With a
+    flush, every step has its own pair and flush() writes a buffer larger than
+    L2 just before it, outside the pair."""
+    if flush is None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+    pairs = []
+    for _ in range(steps):
+        flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        pairs.append((a, b))
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in pairs) / steps
+
+
+def zstd_bit_exact(data, d_seqs, d_off, depth, nsample=512):
+    """Sequences of `nsample` windows spread over the input (first and last
+    included) against the oracle, outside every timed region."""
+    import gcz
+    from oracle import oracle as orc
+
+    n = data.size
+    B = gcz.num_windows(n)
+    idx = np.unique(np.linspace(0, B - 1, min(nsample, B)).astype(np.int64))
+    off = d_off.cpu().numpy().astype(np.int64)
+    got = d_seqs[:int(off[-1])].cpu().numpy().view(np.uint32)
+    sub = np.concatenate([data[i * 65536:(i + 1) * 65536] for i in idx])  # ragged last window stays last
+    o_seqs, o_off = orc.zstd_sequences(sub, depth, threads=os.cpu_count() or 1)
+    o_off = o_off.astype(np.int64)
+    bad = [int(i) for k, i in enumerate(idx)
+           if not np.array_equal(got[off[i]:off[i + 1]], o_seqs[o_off[k]:o_off[k + 1]])]
+    return {"equal": not bad, "windows_checked": int(idx.size), "windows_differing": bad[:8],
+            "sequences_checked": int(o_off[-1]), "against": "oracle/oracle.c (pinned to the reference kernels)"}
+
+
+def zstd_ratio(ctx, data, depth, threads):
+    """Compression ratio of Zstd frames built from these sequences by the
+    reference's own coder loop (ZSTD_compressSequences per 64 KiB window,
+    compress_zstd_custom.rs:115-199) on a sample, next to the same loop fed
+    with the oracle's (= the reference kernels') sequences."""
+    from gcz import codecs
+    from oracle import oracle as orc
+
+    level = 2 if depth > 16 else 1
+    blob, _ = ctx.zstd_compress_frames(data, level, threads)
+    o_seqs, o_off = orc.zstd_sequences(data, depth, threads=threads)
+    comp = codecs.SequenceCompressor()
+    ref = bytearray()
+    for b in range(o_off.size - 1):
+        ref += comp.compress(data[b * 65536:(b + 1) * 65536], o_seqs[int(o_off[b]):int(o_off[b + 1])])
+    comp.close()
+    r, rr = len(blob) / data.size, len(ref) / data.size
+    return {"value": round(r, 5), "reference_value": round(rr, 5), "delta_pp": round(100 * (r - rr), 4),
+            "frames_identical": bytes(blob.tobytes()) == bytes(ref), "sample_bytes": int(data.size),
+            "coder": "libzstd 1.5.5 ZSTD_compressSequences per window (param 1001 = 0, session reset)"}
+
+
+def zstd_config1(ctx, torch, dev, steps, warmup):
+    """Config 1, Zstd L1 plain: one 16 MiB input (seed 1), depth 16.  The input
+    fits in L2, so every timed step follows a 512 MiB write that flushes it.
+    e2e and its per-call latency go through the host-buffer call."""
+    import gcz
+
+    n, depth = 16 << 20, 16
+    data = gcz.gen_synthetic(1, n, 8 << 20)
+    B = gcz.num_windows(n)
+    d_in = torch.from_numpy(data).to(dev)
+    cap = int(gcz.L.gcz_zstd_max_sequences(n))
+    d_seqs = torch.empty((cap, 4), dtype=torch.int32, device=dev)
+    d_off = torch.empty(B + 1, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush_buf = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+
+    def step():
+        ctx.zstd_match_find_device(d_in.data_ptr(), n, depth, d_seqs.data_ptr(), cap, d_off.data_ptr(), sp)
+
+    for _ in range(max(warmup, 3)):
+        step()
+    ctx.sync(sp)
+    nseq = int(d_off[-1].item())
+    ctx.profile_start()
+    ms = time_steps(torch, stream, steps, step, flush=lambda: flush_buf.zero_())
+    kern_ms, kern_launches, _ = ctx.profile_stop()
+    ctx.sync(sp)
+    del flush_buf
+    h_in = torch.from_numpy(data).pin_memory()
+    h_seqs = torch.empty((cap, 4), dtype=torch.int32).pin_memory()
+    h_off = torch.empty(B + 1, dtype=torch.int64).pin_memory()
+
+    def e2e_step():
+        rc = gcz.L.gcz_zstd_match_find(ctx.handle, h_in.data_ptr(), n, depth, h_seqs.data_ptr(), cap,
+                                       h_off.data_ptr())
+        if rc != 0:
+            raise RuntimeError(gcz.L.gcz_last_error(ctx.handle).decode())
+
+    for _ in range(3):
+        e2e_step()
+    lat = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        lat.append((time.perf_counter() - t0) * 1e3)
+    assert int(h_off[-1].item()) == nseq
+    step_ms = kern_ms / max(kern_launches, 1)
+    alg = n + 16 * nseq + 8 * B
+    peak, peak_kind = peaks()
+    return {
+        "workload": "zstd_l1_16mib", "input_bytes": n, "windows": B, "search_depth": depth, "sequences": nseq,
+        "value": round(n / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ms, 4),
+        "value_is": "device-resident, L2 flushed before every step",
+        "e2e": {"value": round(n / (statistics.mean(lat) / 1e3) / 1e9, 3), "unit": "GB/s",
+                "h2d_bytes_per_step": n, "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1)},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3),
+                       "calls": len(lat), "of": "gcz_zstd_match_find on the 16 MiB host buffer"},
+        "roofline": {"bound": "hbm", "achieved": round(alg / (step_ms / 1e3) / 1e9, 1), "peak": peak,
+                     "unit": "GB/s", "frac": round(alg / (step_ms / 1e3) / 1e9 / peak, 4),
+                     "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms_per_step": round(step_ms, 4),
+                     "algorithmic_bytes_per_step": alg},
+        "bit_exact": zstd_bit_exact(data, d_seqs, d_off, depth, nsample=B),
+    }
+
+
 def run_gcz(args):
     import torch
     import gcz
@@ -313,6 +448,7 @@ def run_gcz(args):
 
     # ---- end-to-end through the host-buffer C-ABI call (pinned buffers)
     e2e_value = link_value = None
+    e2e_lat = []
     if args.e2e_steps > 0:
         h_in = torch.from_numpy(data).pin_memory()
         h_seqs = torch.empty((nseq + 1024, 4), dtype=torch.int32).pin_memory()
@@ -328,7 +464,9 @@ def run_gcz(args):
         barrier(dist, torch, local)
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
+            t1 = time.perf_counter()
             e2e_step()
+            e2e_lat.append((time.perf_counter() - t1) * 1e3)
         e2e_s = time.perf_counter() - t0
         barrier(dist, torch, local)
         e2e_max = max_over_ranks(dist, torch, e2e_s)
@@ -336,26 +474,51 @@ def run_gcz(args):
         assert int(h_off[-1].item()) == nseq
         link_s = max_over_ranks(dist, torch, link_time(torch, dev, h_in, d_in, h_seqs, d_seqs, 16 * nseq))
         link_value = round(world * n / link_s / 1e9, 3)
+        del h_in, h_seqs, h_off
 
-    # ---- roofline of the match-find step (match kernel + offset scan + compaction)
+    # ---- roofline of the match-find step (match kernels + offset scan + compaction)
     peak, peak_kind = peaks()
     step_ms = kern_ms / max(kern_launches, 1)
     alg_bytes = n + 16 * nseq + 8 * B  # input once + ZSTD_Sequence out + counts/offsets
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
     traffic = measured_traffic(WORKLOAD, n)
 
-    cpu = libs = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    cpu = libs = exact = ratio = configs = None
+    if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
-        sample = data[:256 << 20]
-        dt, _ = cpu_oracle_time(sample, DEPTH, threads)
-        cpu = {"value": round(sample.size / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": f"first 256 MiB of the same 1 GiB input (4096 windows), oracle/oracle.c on {threads} threads"}
-        libs = cpu_library_baselines(data[:256 << 20], "zstd", threads)
-        small = data[:16 << 20]
-        dt1, _ = cpu_oracle_time(small, DEPTH, 1)
-        libs["oracle single thread"] = {"gbs": round(small.size / dt1 / 1e9, 4), "threads": 1,
-                                        "sample_bytes": int(small.size)}
+        # outside the timed regions: bit-exactness on sampled windows, then the
+        # frames' ratio through the reference's coder loop
+        exact = zstd_bit_exact(data, d_seqs, d_off, DEPTH)
+        ratio = zstd_ratio(ctx, data[:64 << 20], DEPTH, threads)
+        del d_seqs, d_off, d_in
+        torch.cuda.empty_cache()
+        if not args.no_cpu_baseline:
+            sample = data[:256 << 20]
+            dt, _ = cpu_oracle_time(sample, DEPTH, threads)
+            cpu = {"value": round(sample.size / dt / 1e9, 4), "unit": "GB/s", "cores": threads, "kind": "port",
+                   "sample": f"first 256 MiB of the same 1 GiB input (4096 windows), oracle/oracle.c on "
+                             f"{threads} threads"}
+            libs = cpu_library_baselines(data[:256 << 20], "zstd", threads)
+            small = data[:16 << 20]
+            dt1, _ = cpu_oracle_time(small, DEPTH, 1)
+            libs["oracle single thread"] = {"gbs": round(small.size / dt1 / 1e9, 4), "threads": 1,
+                                            "sample_bytes": int(small.size)}
+        if not args.no_configs:
+            # BASELINE's other configs at their stated sizes, each outside the
+            # headline's timed region: 1 (Zstd L1, 16 MiB), 3 (LZMA2 L1, 1 GiB),
+            # 4 (4096 uneven files, ~28 GB), 5 (Poisson serving, 60 s)
+            del data
+            configs = {"zstd_l1_16mib": zstd_config1(ctx, torch, dev, args.steps, args.warmup)}
+            configs["lzma2_l1_1gib"] = measure_lzma2(args, ctx, torch, dev, None, 1, 0, local,
+                                                     cpu_legs=not args.no_cpu_baseline)
+            if not args.no_heavy_configs:
+                with Clocks(local) as c4:
+                    configs["uneven_batch"] = measure_uneven(ctx, torch, args.steps, args.files, args.max_file)
+                configs["uneven_batch"]["clocks"] = c4.summary()
+                with Clocks(local) as c5:
+                    configs["serving"] = measure_serving(ctx, torch, args.rate, args.duration, args.max_request,
+                                                         args.max_batch)
+                configs["serving"]["clocks"] = c5.summary()
 
     total_launches = sum_over_ranks(dist, torch, all_launches)
     if rank == 0:
@@ -363,23 +526,33 @@ def run_gcz(args):
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
+            "value_is": "device-resident: input already in HBM, every match-find kernel of the step, CUDA events "
+                        "on the launch stream; e2e is the same step through the host-buffer call",
             "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "windows_per_gpu": B, "window": 65536,
                        "search_depth": DEPTH, "sequences_per_gpu": nseq, "parallelism": f"replicas{world}",
                        "algo": args.algo, "fallback_windows": ctx.query("fallback_windows"),
                        "l2": "input 1 GiB > 126 MB L2, no flush needed"},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n,
                     "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1),
+                    "call": "gcz_zstd_match_find (pinned host input, ZSTD_Sequence records and offsets back)",
                     "link_bound": {"value": link_value, "unit": "GB/s",
                                    "what": "plain pinned copies of the step's bytes, no kernels: the H2D of the "
                                            "input in 64 MiB pieces with the sequence records' D2H on a second "
                                            "stream"},
                     "frac_of_link": round(e2e_value / link_value, 3) if e2e_value and link_value else None},
+            "latency_ms": ({"p50": round(float(np.percentile(e2e_lat, 50)), 3),
+                            "p99": round(float(np.percentile(e2e_lat, 99)), 3), "calls": len(e2e_lat),
+                            "of": "the 1 GiB host-buffer call (serving latency: --workload serving)"}
+                           if e2e_lat else None),
+            "ratio": ratio,
+            "bit_exact": exact,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_source": f"{peak_kind} hbm_gbs", "kernel_ms_per_step": round(step_ms, 4),
                          "algorithmic_bytes_per_step": alg_bytes},
             "cpu_baseline": cpu,
             "cpu_libraries": libs,
+            "configs": configs,
             "gpu_launches": int(total_launches),
             "clocks": clk.summary(),
         }
@@ -388,16 +561,13 @@ def run_gcz(args):
         dist.destroy_process_group()
 
 
-def run_lzma2(args):
-    """LZMA2 L1 workload: 1 GiB (seed 3, copy offsets to 128 MiB), 16384
-    windows, per-position packed matches + per-window has-match byte."""
-    import torch
+def measure_lzma2(args, ctx, torch, dev, dist, world, rank, local, cpu_legs=True):
+    """Config 3, LZMA2 L1: 1 GiB (seed 3, copy offsets to 128 MiB), 16384
+    windows, per-position packed matches + per-window has-match byte, timed
+    device-resident; e2e through the host-buffer call, both as the triage the
+    encoder consumes and with the per-position results."""
     import gcz
 
-    world, rank, local, dist = dist_setup(args)
-    dev = torch.device("cuda", local)
-    ctx = gcz.Context(local)
-    ctx.set_option("algo", args.algo)
     n = args.bytes
     data = gcz.gen_synthetic(3 + 1000 * rank, n, 128 << 20)
     B = gcz.num_windows(n)
@@ -424,8 +594,23 @@ def run_lzma2(args):
         torch.cuda.synchronize(dev)
         kern_ms, kern_launches, all_launches = ctx.profile_stop()
     barrier(dist, torch, local)
+    ctx.sync(sp)
     ms_max = max_over_ranks(dist, torch, e0.elapsed_time(e1))
     value = world * n * args.steps / (ms_max / 1e3) / 1e9
+    # bit-exact on sampled windows against the oracle, outside the timed region
+    from oracle import oracle as orc
+    idx = np.unique(np.linspace(0, B - 1, min(512, B)).astype(np.int64))
+    got = d_packed.cpu().numpy().view(np.uint32)
+    has = d_has.cpu().numpy()
+    sub = np.concatenate([data[i * 65536:(i + 1) * 65536] for i in idx])
+    o_packed = orc.lzma_packed(sub, 32, threads=os.cpu_count() or 1)
+    o_has = orc.has_matches(o_packed, sub.size)
+    bad = [int(i) for k, i in enumerate(idx)
+           if not np.array_equal(got[i * 65536:i * 65536 + 65536], o_packed[k * 65536:k * 65536 + 65536])
+           or has[i] != o_has[k]]
+    exact = {"equal": not bad, "windows_checked": int(idx.size), "windows_differing": bad[:8],
+             "against": "oracle/oracle.c (pinned to the reference kernels)"}
+    del got
     e2e_value = e2e_packed = None
     if args.e2e_steps > 0:
         h_in = torch.from_numpy(data).pin_memory()
@@ -454,8 +639,11 @@ def run_lzma2(args):
         has_triage = h_has.clone()
         e2e_packed = e2e_run(h_packed.data_ptr())
         assert torch.equal(has_triage, h_has)
+        del h_in, h_packed, h_has
+    del d_in, d_packed, d_has
+    torch.cuda.empty_cache()
     libs = l1 = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and cpu_legs:
         threads = os.cpu_count() or 1
         sample = data[:16 << 20]
         libs = cpu_library_baselines(sample, "lzma2", threads)
@@ -473,62 +661,90 @@ def run_lzma2(args):
     step_ms = kern_ms / max(kern_launches, 1)
     alg_bytes = n + 4 * n + B  # input once + packed matches + has-match bytes
     achieved = alg_bytes / (step_ms / 1e3) / 1e9
+    return {
+        "metric": "input GB/s per B200 (LZMA2 L1 match-find)", "value": round(value, 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator)", "value_is": "device-resident, input 1 GiB > L2",
+        "config": {"workload": "lzma2_l1_1gib", "input_bytes_per_gpu": n, "windows_per_gpu": B, "algo": args.algo},
+        "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": B,
+                "call": "gcz_lzma2_match_find(packed=NULL): per-window has-match bytes"},
+        "e2e_packed": {"value": e2e_packed, "unit": "GB/s", "h2d_bytes_per_step": n,
+                       "d2h_bytes_per_step": 4 * n + B, "call": "gcz_lzma2_match_find: per-position matches"},
+        "bit_exact": exact,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": measured_traffic("lzma2_l1_1gib", n),
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "kernel_ms_per_step": round(step_ms, 4), "algorithmic_bytes_per_step": alg_bytes},
+        "cpu_libraries": libs, "lzma2_l1_nvlz_end_to_end": l1,
+        "gpu_launches": int(all_launches), "clocks": clk.summary()}
+
+
+def run_lzma2(args):
+    """LZMA2 L1 workload on its own line (config 3)."""
+    import torch
+    import gcz
+
+    world, rank, local, dist = dist_setup(args)
+    dev = torch.device("cuda", local)
+    ctx = gcz.Context(local)
+    ctx.set_option("algo", args.algo)
+    line = measure_lzma2(args, ctx, torch, dev, dist, world, rank, local, cpu_legs=not args.no_cpu_baseline)
     if rank == 0:
-        print(json.dumps({
-            "metric": "input GB/s per B200 (LZMA2 L1 match-find)", "value": round(value, 3), "unit": "GB/s",
-            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(ms_max / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic (seeded generator)",
-            "config": {"workload": "lzma2_l1_1gib", "input_bytes_per_gpu": n, "windows_per_gpu": B, "algo": args.algo},
-            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": B,
-                    "call": "gcz_lzma2_match_find(packed=NULL): per-window has-match bytes"},
-            "e2e_packed": {"value": e2e_packed, "unit": "GB/s", "h2d_bytes_per_step": n,
-                           "d2h_bytes_per_step": 4 * n + B, "call": "gcz_lzma2_match_find: per-position matches"},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": measured_traffic("lzma2_l1_1gib", n),
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "kernel_ms_per_step": round(step_ms, 4), "algorithmic_bytes_per_step": alg_bytes},
-            "cpu_libraries": libs, "lzma2_l1_nvlz_end_to_end": l1,
-            "gpu_launches": int(all_launches), "clocks": clk.summary()}), flush=True)
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 
 
-def run_serving(args):
-    """Open-loop Poisson stream against the library's request loop: request
-    sizes log-uniform 4 KiB..max_request, 70% Zstd L1 / 20% Zstd L2 / 10% LZMA2
-    L1, payloads are slices of a pinned 1 GiB synthetic pool.  Reports the
-    completed input GB/s and submit-to-completion p50/p99 latency."""
+def fill_pool(pool_np, seed, block=16 << 20):
+    """A pinned payload pool of `block`-sized spans, each from the generator
+    with its own Dirichlet(1,1,1) mix (Markov / copy / random fractions)."""
+    import gcz
+    from concurrent.futures import ThreadPoolExecutor
+
+    n = pool_np.size
+    nblk = (n + block - 1) // block
+    mixes = np.random.default_rng(seed).dirichlet([1, 1, 1], size=nblk)
+
+    def gen(i):
+        o = i * block
+        gcz.gen_synthetic(seed * 100003 + i, min(block, n - o), 8 << 20, tuple(mixes[i]), out=pool_np[o:o + block])
+
+    with ThreadPoolExecutor(os.cpu_count() or 4) as ex:
+        list(ex.map(gen, range(nblk)))
+
+
+def measure_serving(ctx, torch, rate, duration, max_request, max_batch, budget=120 * 10**9, pool_bytes=4 << 30):
+    """Config 5, serving: an open-loop Poisson stream against the request loop.
+    Request sizes log-uniform 4 KiB..max_request, 70% Zstd L1 / 20% Zstd L2 /
+    10% LZMA2 L1 (has-match bytes, what the LZMA2 encoder reads).  Payloads are
+    slices of a pinned pool made of 16 MiB spans with their own Dirichlet mix;
+    results go to a pinned ring freed in completion order.  Reports offered and
+    served GB/s and the submit-to-completion p50/p99 the loop measured."""
     import threading
-    import torch
     import gcz
     from gcz import serving
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    ctx = gcz.Context(local)
-    pool_n = 1 << 30
-    pool = torch.empty(pool_n, dtype=torch.uint8, pin_memory=True)
-    gcz.gen_synthetic(5, pool_n, 8 << 20, out=pool.numpy())
-    srv = serving.Server(ctx, hbm_budget=120 * 10**9, max_batch_bytes=args.max_batch)
+    pool = torch.empty(pool_bytes, dtype=torch.uint8, pin_memory=True)
+    pool_np = pool.numpy()
+    fill_pool(pool_np, 5)
+    srv = serving.Server(ctx, hbm_budget=budget, max_batch_bytes=max_batch)
+    slots, dev_bytes = srv.info()
     rng = np.random.default_rng(11)
-    count = int(args.rate * args.duration)
-    gaps = rng.exponential(1.0 / args.rate, size=count)
-    sizes = np.exp(rng.uniform(np.log(4096), np.log(args.max_request), size=count)).astype(np.int64)
+    count = int(rate * duration)
+    gaps = rng.exponential(1.0 / rate, size=count)
+    sizes = np.exp(rng.uniform(np.log(4096), np.log(max_request), size=count)).astype(np.int64)
     u = rng.random(count)
     kinds = np.where(u < 0.9, serving.ZSTD, serving.LZMA2)
     depths = np.where(u < 0.7, 16, np.where(u < 0.9, 64, 32))
-    offs = (rng.random(count) * (pool_n - sizes)).astype(np.int64)
-    pool_np = pool.numpy()
+    offs = (rng.random(count) * (pool_bytes - sizes)).astype(np.int64)
     q = []
     lock = threading.Condition()
-    # Outputs go to one pinned ring, allocated in submission order and freed in
-    # completion order (the waiter completes requests in order); a full ring
-    # holds the submitter back.  Zstd results get room for n/16 + 1024
-    # sequences (this input averages one sequence per ~50 bytes).
-    ring_n = 4 << 30
+    # Zstd results get room for n/16 + 1024 sequences (this input averages one
+    # sequence per ~50 bytes); a full ring holds the submitter back.
+    ring_n = 8 << 30
     ring = torch.empty(ring_n, dtype=torch.uint8, pin_memory=True).numpy()
-    rs = {"head": 0, "tail": 0}
+    rs = {"head": 0, "tail": 0, "stalls": 0}
     ring_cv = threading.Condition()
 
     def ring_alloc(nbytes):
@@ -537,6 +753,8 @@ def run_serving(args):
             h = rs["head"]
             if h % ring_n + nbytes > ring_n:
                 h += ring_n - h % ring_n  # skip the ring's end
+            if h + nbytes - rs["tail"] > ring_n:
+                rs["stalls"] += 1
             while h + nbytes - rs["tail"] > ring_n:
                 ring_cv.wait()
             rs["head"] = h + nbytes
@@ -562,31 +780,20 @@ def run_serving(args):
             q[i] = None
             i += 1
 
-    # Warm-up outside the timed region: two largest batches of each kind, so both
-    # slots of the loop hold their device buffers at full size.  The loop flips
-    # slots on every batch, so the two of a kind go back to back (Z, Z, L, L);
-    # alternating kinds would leave each slot warm for one kind only, and the
-    # other kind's first batches there would allocate inside the timed region.
-    wn = min(args.max_batch, pool_n)
-    for kind in (serving.ZSTD, serving.ZSTD, serving.LZMA2, serving.LZMA2):
-        if kind == serving.ZSTD:
-            cap = wn // 16 + 1024
-            r = srv.submit(kind, pool_np[:wn], 16, out_a=ring[:cap * 16].view(np.uint32).reshape(cap, 4), cap=cap,
-                           out_b=ring[cap * 16:cap * 16 + (gcz.num_windows(wn) + 1) * 8].view(np.uint64))
-        else:
-            r = srv.submit(kind, pool_np[:wn], 32, out_b=ring[:gcz.num_windows(wn)], packed=False)
-        srv.wait(r)
+    srv.warm_up((serving.ZSTD, serving.LZMA2))
     base = srv.stats()
-
     wt = threading.Thread(target=waiter)
     wt.start()
     t0 = time.perf_counter()
     nxt = t0
+    late = 0.0
     for i in range(count):
         nxt += gaps[i]
         d = nxt - time.perf_counter()
         if d > 0:
             time.sleep(d)
+        else:
+            late = max(late, -d)
         n = int(sizes[i])
         nb = gcz.num_windows(n)
         if kinds[i] == serving.ZSTD:
@@ -602,120 +809,190 @@ def run_serving(args):
         with lock:
             q.append((r, end))
             lock.notify()
+    t_sub = time.perf_counter() - t0
     wt.join()
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    done_bytes = st["bytes"] - base["bytes"]
-    st["batches"] -= base["batches"]
-    st["completed"] -= base["completed"]
-    st["p50_ms"], st["p99_ms"] = float(np.percentile(lats, 50)), float(np.percentile(lats, 99))
-    print(json.dumps({
-        "metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "value": round(done_bytes / wall / 1e9, 3),
-        "unit": "GB/s", "n_gpus": 1, "higher_is_better": True, "dtype": "u8", "data": "synthetic (seeded pool)",
-        "config": {"workload": "serving_poisson", "rate_per_s": args.rate, "duration_s": args.duration,
-                   "requests": count, "size_range": [4096, args.max_request], "mix": "70% zstd L1, 20% zstd L2, 10% lzma2 (has-match bytes only)",
-                   "outputs": "pinned 4 GiB ring, freed in completion order", "offered_gbps": round(float(sizes.sum()) / args.duration / 1e9, 3), "hbm_budget_bytes": 120 * 10**9,
-                   "max_batch_bytes": args.max_batch},
-        "latency_ms": {"p50": round(st["p50_ms"], 3), "p99": round(st["p99_ms"], 3)},
-        "batches": st["batches"], "completed": st["completed"], "wall_s": round(wall, 3)}), flush=True)
+    del ring, pool
+    done = st["bytes"] - base["bytes"]
+    return {
+        "workload": "serving_poisson", "value": round(done / wall / 1e9, 3), "unit": "GB/s",
+        "value_is": "input bytes completed / wall time from the first arrival to the last completion",
+        "offered_gbs": round(float(sizes.sum()) / duration / 1e9, 3),
+        "latency_ms": {"p50": round(float(np.percentile(lats, 50)), 3), "p99": round(float(np.percentile(lats, 99)), 3),
+                       "max": round(float(lats.max()), 3), "of": "submit to completion, every request"},
+        "rate_per_s": rate, "duration_s": duration, "requests": count, "size_range": [4096, max_request],
+        "mix": "70% Zstd L1, 20% Zstd L2, 10% LZMA2 L1 (has-match bytes); 16 MiB pool spans with Dirichlet(1,1,1) mixes",
+        "hbm_budget_bytes": budget, "max_batch_bytes": max_batch, "slots": slots, "device_bytes_held": dev_bytes,
+        "batches": st["batches"] - base["batches"], "completed": st["completed"] - base["completed"],
+        "submit_seconds": round(t_sub, 3), "wall_s": round(wall, 3), "ring_stalls": rs["stalls"],
+        "max_submit_lag_s": round(late, 4), "status": st["status"]}
 
 
-def run_uneven(args):
-    """Uneven batch: many files of log-uniform size with per-file Dirichlet(1,1,1)
-    mixes in one launch through the window-table entry point (device resident).
-    Reports input GB/s of the launch."""
+def run_serving(args):
+    """Config 5 on its own line (see measure_serving)."""
     import torch
     import gcz
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     ctx = gcz.Context(local)
-    sizes, mix = gcz.gen_file_sizes(4, args.files, 4096, args.max_file)
-    foff, wins, slab = gcz.batch_layout(sizes)
-    h_slab = torch.zeros(slab, dtype=torch.uint8).pin_memory()
-    hs = h_slab.numpy()
+    with Clocks(local) as clk:
+        res = measure_serving(ctx, torch, args.rate, args.duration, args.max_request, args.max_batch)
+    line = {"metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "u8", "data": "synthetic (seeded pool)", **res,
+            "config": {"workload": "serving_poisson"}, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def measure_uneven(ctx, torch, steps, files=4096, max_file=64 << 20, part_windows=32768):
+    """Config 4, uneven batch: `files` files of log-uniform size 4 KiB..max_file
+    with per-file Dirichlet(1,1,1) mixes, Zstd L1 (depth 16), device-resident.
+    The slab does not fit one launch's scratch at 18 device bytes per input
+    byte, so its window table is cut into parts of at most `part_windows`
+    windows; all parts' launches are captured in one CUDA graph, and a step is
+    one replay of it (every window of every file)."""
+    import gcz
     from concurrent.futures import ThreadPoolExecutor
 
-    def gen(i):
-        o, sz = int(foff[i]), int(sizes[i])
-        gcz.gen_synthetic(4000 + i, sz, 8 << 20, tuple(mix[i]), out=hs[o:o + sz])
-
+    sizes, mix = gcz.gen_file_sizes(4, files, 4096, max_file)
+    foff, wins, slab = gcz.batch_layout(sizes)
+    total = int(np.sum(sizes))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_slab = torch.empty(slab + 64, dtype=torch.uint8, device=dev)
+    # generate file by file into a pinned staging buffer, copy into the slab
+    stage_n = 1 << 30
+    stage = torch.empty(stage_n, dtype=torch.uint8, pin_memory=True)
+    st_np = stage.numpy()
+    order = np.argsort(foff)
+    i = 0
     with ThreadPoolExecutor(os.cpu_count() or 4) as ex:
-        list(ex.map(gen, range(len(sizes))))
-    d_slab = h_slab.cuda()
-    d_wins = torch.from_numpy(wins.view(np.uint8)).cuda()
-    cap = sum(int(gcz.L.gcz_zstd_max_sequences(int(x))) for x in sizes)
-    d_seqs = torch.empty((cap, 4), dtype=torch.int32, device="cuda")
-    d_off = torch.empty(wins.size + 1, dtype=torch.int64, device="cuda")
+        while i < len(order):
+            j, used, jobs = i, 0, []
+            while j < len(order) and (used + int(sizes[order[j]]) <= stage_n or j == i):
+                f = int(order[j])
+                jobs.append((f, used))
+                used += (int(sizes[f]) + 15) & ~15
+                j += 1
+            list(ex.map(lambda fu: gcz.gen_synthetic(4000 + fu[0], int(sizes[fu[0]]), 8 << 20, tuple(mix[fu[0]]),
+                                                     out=st_np[fu[1]:fu[1] + int(sizes[fu[0]])]), jobs))
+            for f, u in jobs:
+                o, sz = int(foff[f]), int(sizes[f])
+                d_slab[o:o + sz].copy_(stage[u:u + sz], non_blocking=True)
+            torch.cuda.synchronize()
+            i = j
+    del stage, st_np
+    # parts: contiguous window ranges, offsets rebased to the part's first byte
+    parts = []
+    for w0 in range(0, wins.size, part_windows):
+        w1 = min(wins.size, w0 + part_windows)
+        pw = wins[w0:w1].copy()
+        base = int(pw["offset"][0])
+        pw["offset"] -= base
+        pbytes = int(pw["offset"][-1]) + int(pw["size"][-1])
+        cap = sum(int(gcz.L.gcz_zstd_max_sequences(int(x))) for x in pw["size"]) // 4 + 1024
+        parts.append({"base": base, "bytes": pbytes, "wins": torch.from_numpy(pw.view(np.uint8)).to(dev),
+                      "n": int(pw.size), "cap": cap,
+                      "seqs": torch.empty((cap, 4), dtype=torch.int32, device=dev),
+                      "off": torch.empty(int(pw.size) + 1, dtype=torch.int64, device=dev)})
     st = torch.cuda.current_stream()
 
-    def step():
-        ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16,
-                                         d_seqs.data_ptr(), cap, d_off.data_ptr(), st.cuda_stream)
+    def launch_all(stream):
+        for p in parts:
+            ctx.zstd_match_find_batch_device(d_slab.data_ptr() + p["base"], p["bytes"], p["wins"].data_ptr(), p["n"],
+                                             16, p["seqs"].data_ptr(), p["cap"], p["off"].data_ptr(), stream)
 
-    for _ in range(3):  # also sizes every buffer, so the captured launches allocate nothing
-        step()
+    for _ in range(3):  # also sizes every scratch buffer, so the captured launches allocate nothing
+        launch_all(st.cuda_stream)
     ctx.sync(st.cuda_stream)
-    # the whole batch as one CUDA graph (the launches of one match-find step)
+    nseq = sum(int(p["off"][-1].item()) for p in parts)
     cs = torch.cuda.Stream()
     g = torch.cuda.CUDAGraph()
     with torch.cuda.stream(cs):
         with torch.cuda.graph(g, stream=cs):
-            ctx.zstd_match_find_batch_device(d_slab.data_ptr(), slab, d_wins.data_ptr(), wins.size, 16,
-                                             d_seqs.data_ptr(), cap, d_off.data_ptr(), cs.cuda_stream)
+            launch_all(cs.cuda_stream)
     torch.cuda.synchronize()
     g.replay()
     torch.cuda.synchronize()
     ctx.sync(st.cuda_stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    for _ in range(args.steps):
-        g.replay()
-    e1.record(st)
-    torch.cuda.synchronize()
+    ms = time_steps(torch, st, steps, g.replay)
     ctx.sync(st.cuda_stream)
-    ms = e0.elapsed_time(e1) / args.steps
-    total = int(np.sum(sizes))
-    print(json.dumps({
-        "metric": "uneven-batch input GB/s per B200 (Zstd L1 match-find, one launch)",
-        "value": round(total / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ms, 3),
-        "config": {"workload": "uneven_batch", "files": args.files, "size_range": [4096, args.max_file],
-                   "input_bytes": total, "windows": int(wins.size), "mix": "Dirichlet(1,1,1) per file",
-                   "launch": "one CUDA graph replay per step"}}), flush=True)
+    # one small file and the largest file against the oracle, outside the timed region
+    from oracle import oracle as orc
+    checked = []
+    first_win = np.searchsorted(wins["offset"], foff)
+    nwins = np.array([gcz.num_windows(int(x)) for x in sizes])
+    inside = (first_win // part_windows) == ((first_win + nwins - 1) // part_windows)  # not cut by a part boundary
+    by_size = [int(f) for f in np.argsort(sizes) if inside[f]]
+    for f in (by_size[0], by_size[-1]):  # the smallest and the largest file that one part holds whole
+        w_first, nwf = int(first_win[f]), int(nwins[f])
+        k = w_first // part_windows
+        p = parts[k]
+        lw = w_first - k * part_windows
+        off = p["off"].cpu().numpy().astype(np.int64)
+        got = p["seqs"][off[lw]:off[lw + nwf]].cpu().numpy().view(np.uint32)
+        data = d_slab[int(foff[f]):int(foff[f]) + int(sizes[f])].cpu().numpy()
+        o_seqs, _ = orc.zstd_sequences(data, 16, threads=os.cpu_count() or 1)
+        checked.append({"file": f, "bytes": int(sizes[f]), "equal": bool(np.array_equal(got, o_seqs))})
+    res = {"workload": "uneven_batch", "value": round(total / (ms / 1e3) / 1e9, 3), "unit": "GB/s",
+           "ms_per_step": round(ms, 3), "value_is": "device-resident, one CUDA graph replay per step",
+           "files": files, "size_range": [4096, max_file], "input_bytes": total, "slab_bytes": int(slab),
+           "windows": int(wins.size), "launch_parts": len(parts), "part_windows": part_windows,
+           "sequences": nseq, "mix": "Dirichlet(1,1,1) per file", "search_depth": 16,
+           "bit_exact": {"equal": all(c["equal"] for c in checked), "files_checked": checked,
+                         "against": "oracle/oracle.c"}}
+    del parts, d_slab, g
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_uneven(args):
+    """Config 4 on its own line (see measure_uneven)."""
+    import torch
+    import gcz
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = gcz.Context(local)
+    with Clocks(local) as clk:
+        res = measure_uneven(ctx, torch, args.steps, args.files, args.max_file)
+    print(json.dumps({"metric": "uneven-batch input GB/s per B200 (Zstd L1 match-find)", **res,
+                      "config": {"workload": "uneven_batch"}, "clocks": clk.summary()}), flush=True)
 
 
 def run_reference(args):
-    """Reference arm: the reference's path on this box.  `value` = its CPU
-    restatement (oracle port) on all host threads over a bounded sample of the
-    workload; `reference_kernels_b200` = the reference's own kernels on the GPU."""
+    """Reference arm: the reference's path on this box, on the same workload
+    (1 GiB, seed 2, depth 64), the same --steps/--warmup and the same metric.
+    The reference has no CPU match finder, so `value` is its kernels' CPU
+    restatement (the oracle port) on all host threads over the whole 1 GiB per
+    step; `reference_kernels_b200` times the reference's own kernels (PTX from
+    its sources, driver JIT) on the same GPU.  Nothing here loads libgcz.so:
+    the input comes from the oracle's own build of the generator."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import gcz
+    from oracle import oracle as orc
 
-    n = N_BYTES
-    data = gcz.gen_synthetic(SEED, n, 8 << 20)
+    n = args.bytes
+    data = orc.gen_synthetic(SEED, n, 8 << 20)
     threads = os.cpu_count() or 1
-    sample = data[:256 << 20]
-    times = []
-    for _ in range(max(args.warmup, 1)):
-        cpu_oracle_time(sample[:16 << 20], DEPTH, threads)
-    steps = max(1, min(args.steps, 5))
-    for _ in range(steps):
-        dt, _ = cpu_oracle_time(sample, DEPTH, threads)
-        times.append(dt)
-    value = sample.size * steps / sum(times) / 1e9
+    for _ in range(max(args.warmup, 3)):
+        cpu_oracle_time(data, DEPTH, threads)
+    times = [cpu_oracle_time(data, DEPTH, threads)[0] for _ in range(args.steps)]
+    value = n * len(times) / sum(times) / 1e9
     refk = reference_kernels(data)
     line = {
-        "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": steps,
-        "warmup": max(args.warmup, 1), "ms_per_step": round(sum(times) / steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
-        "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "window": 65536, "search_depth": DEPTH},
+        "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(sum(times) / len(times) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "windows_per_gpu": (n + 65535) // 65536,
+                   "window": 65536, "search_depth": DEPTH},
         "impl": "reference",
         "cpu_baseline": {"value": round(value, 4), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"first 256 MiB of the 1 GiB input, oracle/oracle.c on {threads} threads "
+                         "sample": f"the whole {n >> 20} MiB input every step, oracle/oracle.c on {threads} threads "
                                    "(the reference has no CPU match finder; its kernels are timed below)"},
         "e2e": {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_kernels_b200": refk,
@@ -724,11 +1001,18 @@ def run_reference(args):
 
 
 def reference_kernels(data):
-    """The reference's zstd_match_find PTX (JIT on this GPU) over the same
-    1 GiB in one grid (kernel only), and its adapter pattern per 8 MiB chunk
-    (alloc_zeros + H2D + launch + D2H of the sequence buffer) on a sample."""
+    """The reference's own kernels (PTX from its sources and flags, JIT on this
+    GPU, grid = windows, block = 256) on the same bytes:
+    - zstd_match_find over the whole input in one grid (kernel only), and its
+      adapter pattern per 8 MiB chunk (alloc_zeros + H2D + launch + D2H of the
+      sequence buffer, compress_zstd_custom.rs:79-116) on 128 MiB;
+    - lzma2_match_find per 128 MiB pipeline chunk (pipeline_lzma2.rs:116-190)
+      over the LZMA2 input (seed 3, offsets to 128 MiB), kernel only, and its
+      adapter pattern (alloc_zeros of 64 B + 4 B per byte, H2D, launch, D2H of
+      both buffers, compress_lzma2_custom.rs:508-540) on one chunk."""
     try:
         from oracle import ref_kernels
+        from oracle import oracle as orc
         import torch
 
         if not ref_kernels.available() or not torch.cuda.is_available():
@@ -747,7 +1031,6 @@ def reference_kernels(data):
         k_ms = e0.elapsed_time(e1)
         del bufs, d_in
         torch.cuda.empty_cache()
-        # adapter pattern, 8 MiB chunks (compress_zstd_custom.rs:79-116), first 128 MiB
         chunk = 8 << 20
         sample = data[:128 << 20]
         t0 = time.perf_counter()
@@ -760,9 +1043,46 @@ def reference_kernels(data):
             b[2].cpu()
         torch.cuda.synchronize()
         a_s = time.perf_counter() - t0
-        return {"kernel_only_gbs": round(n / (k_ms / 1e3) / 1e9, 4), "kernel_ms_1gib": round(k_ms, 3),
-                "adapter_pattern_gbs": round(sample.size / a_s / 1e9, 4),
-                "note": "PTX from the reference's own sources and flags, driver JIT; grid=windows, block=256"}
+        res = {"zstd_kernel_only_gbs": round(n / (k_ms / 1e3) / 1e9, 4), "zstd_kernel_ms": round(k_ms, 3),
+               "zstd_adapter_pattern_gbs": round(sample.size / a_s / 1e9, 4),
+               "note": "PTX from the reference's own sources and flags, driver JIT; grid = windows, block = 256"}
+        del sample
+        torch.cuda.empty_cache()
+        # LZMA2: 128 MiB chunks, one 8.5 GiB output allocation reused for the kernel-only timing
+        lz = orc.gen_synthetic(3, n, 128 << 20)
+        lchunk = 128 << 20
+        lb = rk.lzma_alloc(min(lchunk, n))
+        d = rk.to_device(lz[:lchunk])
+        rk.lzma_launch(d, min(lchunk, n), lb)  # JIT + warm-up
+        torch.cuda.synchronize()
+        l_ms = 0.0
+        for off in range(0, n, lchunk):
+            part = lz[off:off + lchunk]
+            d = rk.to_device(part)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            rk.lzma_launch(d, part.size, lb)
+            b.record()
+            torch.cuda.synchronize()
+            l_ms += a.elapsed_time(b)
+        del lb, d
+        torch.cuda.empty_cache()
+        t0 = time.perf_counter()
+        part = lz[:lchunk]
+        d = rk.to_device(part)
+        b = rk.lzma_alloc(part.size)
+        rk.lzma_launch(d, part.size, b)
+        b[0].cpu()
+        b[1].cpu()
+        torch.cuda.synchronize()
+        la_s = time.perf_counter() - t0
+        del b, d
+        torch.cuda.empty_cache()
+        res.update({"lzma2_kernel_only_gbs": round(n / (l_ms / 1e3) / 1e9, 4), "lzma2_kernel_ms": round(l_ms, 3),
+                    "lzma2_adapter_pattern_gbs": round(part.size / la_s / 1e9, 4),
+                    "lzma2_note": "8 launches of 128 MiB (2048 windows each) over the 1 GiB LZMA2 input; the "
+                                  "adapter pattern moves 8.5 GiB of zero-filled slots and counts back per chunk"})
+        return res
     except Exception as e:  # report, never fail the arm
         return {"unavailable": f"{type(e).__name__}: {e}"}
 

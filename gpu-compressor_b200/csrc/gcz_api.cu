@@ -1127,11 +1127,17 @@ double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Worst-case device bytes per input byte of one batch: slab 1, candidates 2,
-// Zstd packed 2.67, speculative lists 3.25, ZSTD_Sequence output 5.33, and
-// for frames requests the frames 1.02, frame slots 1.02, offset codes 1.33
-// and plans 0.03.
-constexpr double kDeviceBytesPerInputByte = 18.0;
+// Device bytes per input byte of one slot, pre-sized at creation for a batch of
+// max_batch_bytes of any mix of kinds: slab 1, candidates 2, Zstd speculative
+// lists 3.25, packed sequences 2.67, ZSTD_Sequence output 5.33, LZMA2 packed
+// matches 4, and for frames the frames 1.02, frame slots 1.02, offset codes
+// 1.33 and plans 0.03.
+constexpr double kDeviceBytesPerInputByte = 22.0;
+constexpr int kMaxServerSlots = 8;
+
+// Request groups, in window order inside a batch: every group's windows are one
+// contiguous range of the batch's window table, so each runs as one launch.
+enum { kGrpSeqLazy = 0, kGrpSeqGreedy, kGrpFramesLazy, kGrpFramesGreedy, kGrpLzma, kGroups };
 
 struct ServerReq {
     uint64_t id = 0;
@@ -1145,25 +1151,47 @@ struct ServerReq {
     double t_submit = 0, t_admit = 0, t_done = 0;
     int status = 1;  // 1 = pending; written under the server's mutex only (waiters read it there)
     int fail = 0;    // the worker's own note of this request's failure, published as status on completion
+    int group = 0;
     uint32_t w0 = 0, nw = 0;
     uint64_t slab_off = 0;
+    uint32_t selftest_iters = 0;  // > 0: a failure-detection probe (gcz_server_selftest_wait_timeout)
 };
 
-struct Batch {
+int req_group(const ServerReq *q) {
+    const bool lazy = q->depth > 1;
+    if (q->kind == GCZ_REQ_ZSTD) return lazy ? kGrpSeqLazy : kGrpSeqGreedy;
+    if (q->kind == GCZ_REQ_ZSTD_FRAMES) return lazy ? kGrpFramesLazy : kGrpFramesGreedy;
+    return kGrpLzma;
+}
+
+}  // namespace
+
+namespace {
+// One batch in flight: its stream, its own status words and every device
+// buffer a max_batch_bytes batch of any mix of kinds needs, allocated once at
+// creation (so serving never calls cudaMalloc or cudaFree).
+struct ServerSlot {
+    gcz_server *sv = nullptr;
+    int index = 0;
+    cudaStream_t st = nullptr;
+    DevBuf in, wins, status, cand, seg, packed, counts, offsets, seqs, lz_packed, lz_has, frames, foff;
+    DevBuf zslots, zovs, zaux, zplan;
+    HostBuf h_off, h_foff, h_status;
+    std::vector<gcz_window> hwins;
     std::vector<ServerReq *> reqs;
-    int kind = 0;
-    uint32_t depth = 0;
-    uint32_t nb = 0;
-    int err = 0;  // status of the batch's launch (GCZ_OK or why it failed part-way)
-    bool busy = false;
+    uint32_t wb[kGroups + 1] = {};  // window bounds of the groups
+    int phase = 0;                  // 0 free, 1 kernels and fixed-size copies queued, 2 result copies queued
+    bool signaled = false;          // the queued phase has finished on the GPU (host callback)
+    int err = GCZ_OK;
 };
-
 }  // namespace
 
 struct gcz_server {
     gcz_ctx *c = nullptr;
     uint64_t max_batch_bytes = 0;
     uint32_t max_batch_requests = 0;
+    uint64_t device_bytes = 0;
+    int nslots = 0;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::deque<ServerReq *> pending;
@@ -1171,170 +1199,278 @@ struct gcz_server {
     uint64_t next_id = 1;
     bool stop = false;
     std::thread worker;
-    Slot slots[2];
-    DevBuf wins[2];
-    std::vector<gcz_window> hwins[2];
-    Batch batch[2];
+    ServerSlot slots[kMaxServerSlots];
     // Latencies of the most recent kLatWindow completed requests (a ring once
     // full), so that a long-running loop's memory and stats cost stay bounded.
     static constexpr size_t kLatWindow = size_t(1) << 20;
     std::vector<double> lat_ms;
     size_t lat_next = 0;
-    uint64_t completed = 0, bytes_done = 0, batches = 0;
+    uint64_t completed = 0, bytes_done = 0, batches = 0, max_in_flight = 0;
     int worker_error = GCZ_OK;
 };
 
 namespace {
 
-// Enqueue one batch on its slot: H2D of every request, the window table, the
-// match-find kernels and the copies whose sizes are already known.
-int server_launch(gcz_server *sv, int k) {
+// Runs on a CUDA callback thread when a slot's queued work has finished: only
+// flags the slot and wakes the worker (no CUDA calls are allowed here).
+void CUDART_CB slot_signal(void *p) {
+    ServerSlot *s = static_cast<ServerSlot *>(p);
+    {
+        std::lock_guard<std::mutex> lk(s->sv->mu);
+        s->signaled = true;
+    }
+    s->sv->cv_work.notify_one();
+}
+
+int slot_alloc(gcz_ctx *c, ServerSlot &s, uint64_t max_bytes) {
+    const size_t W = max_bytes / kW;  // admission counts whole windows, so a batch has at most W
+    int r;
+    const size_t seq_cap = W * (size_t)kMaxSeqs;
+    const size_t fbound = gcz_zstd_frames_bound(max_bytes);
+    struct {
+        DevBuf *b;
+        size_t bytes;
+    } dev[] = {{&s.in, max_bytes + 64},
+               {&s.wins, W * sizeof(gcz_window) + 64},
+               {&s.status, 256},
+               {&s.cand, max_bytes * 2 + 64},
+               {&s.seg, gcz::zstd2_seg_scratch_entries((uint32_t)W) * 8},
+               {&s.packed, seq_cap * 8},
+               {&s.counts, W * 4 + 64},
+               {&s.offsets, (W + 1) * 8},
+               {&s.seqs, seq_cap * 16},
+               {&s.lz_packed, max_bytes * 4 + 64},
+               {&s.lz_has, W + 64},
+               {&s.frames, fbound},
+               {&s.foff, (W + 1) * 8},
+               {&s.zslots, W * (size_t)gcz::kZencSlot},
+               {&s.zovs, W * (size_t)gcz::kZencMaxSeqs * 4},
+               {&s.zaux, W * 12 + 64},
+               {&s.zplan, W * ((size_t)gcz::kZencPlanBytes + 1024)}};
+    for (auto &d : dev)
+        if ((r = ensure_dev(c, *d.b, d.bytes)) != GCZ_OK) return r;
+    if ((r = ensure_host(c, s.h_off, (W + 1) * 8)) != GCZ_OK) return r;
+    if ((r = ensure_host(c, s.h_foff, (W + 1) * 8)) != GCZ_OK) return r;
+    if ((r = ensure_host(c, s.h_status, 64)) != GCZ_OK) return r;
+    return GCZ_OK;
+}
+
+void slot_release(ServerSlot &s) {
+    for (DevBuf *b : {&s.in, &s.wins, &s.status, &s.cand, &s.seg, &s.packed, &s.counts, &s.offsets, &s.seqs,
+                      &s.lz_packed, &s.lz_has, &s.frames, &s.foff, &s.zslots, &s.zovs, &s.zaux, &s.zplan})
+        if (b->p) {
+            cudaFree(b->p);
+            b->p = nullptr;
+            b->cap = 0;
+        }
+    for (HostBuf *b : {&s.h_off, &s.h_foff, &s.h_status})
+        if (b->p) {
+            cudaFreeHost(b->p);
+            b->p = nullptr;
+            b->cap = 0;
+        }
+    if (s.st) cudaStreamDestroy(s.st);
+    s.st = nullptr;
+}
+
+// Enqueue one batch on its slot: the H2D of every request, the window table,
+// one candidate sweep over all windows, then per group the second stage (Zstd
+// parse, lazy and greedy; GPU frames; LZMA2 verification), the copies whose
+// sizes are known already, the status words, and the signal.
+int server_launch(gcz_server *sv, ServerSlot &s) {
     gcz_ctx *c = sv->c;
-    Batch &b = sv->batch[k];
-    Slot &sl = sv->slots[k];
-    std::vector<gcz_window> &hw = sv->hwins[k];
+    std::stable_sort(s.reqs.begin(), s.reqs.end(),
+                     [](const ServerReq *a, const ServerReq *b) { return a->group < b->group; });
     std::vector<size_t> sizes;
-    for (ServerReq *r : b.reqs) sizes.push_back(r->n);
+    for (ServerReq *r : s.reqs) sizes.push_back(r->n);
     std::vector<uint64_t> foff(sizes.size());
     const size_t nb = gcz_batch_num_windows(sizes.data(), sizes.size());
-    hw.resize(nb);
+    s.hwins.resize(nb);
     uint64_t slab = 0;
-    gcz_batch_layout(sizes.data(), sizes.size(), foff.data(), hw.data(), &slab);
+    gcz_batch_layout(sizes.data(), sizes.size(), foff.data(), s.hwins.data(), &slab);
     uint32_t w = 0;
-    for (size_t i = 0; i < b.reqs.size(); i++) {
-        b.reqs[i]->slab_off = foff[i];
-        b.reqs[i]->w0 = w;
-        b.reqs[i]->nw = (uint32_t)nwin(sizes[i]);
-        w += b.reqs[i]->nw;
+    for (int g = 0; g <= kGroups; g++) s.wb[g] = 0;
+    for (size_t i = 0; i < s.reqs.size(); i++) {
+        ServerReq *q = s.reqs[i];
+        q->slab_off = foff[i];
+        q->w0 = w;
+        q->nw = (uint32_t)nwin(sizes[i]);
+        w += q->nw;
+        s.wb[q->group + 1] = w;
     }
-    b.nb = (uint32_t)nb;
+    for (int g = 1; g <= kGroups; g++) s.wb[g] = std::max(s.wb[g], s.wb[g - 1]);
     std::lock_guard<std::mutex> lk(c->mu);
-    DeviceGuard g(c->device);
-    int r;
-    if ((r = ensure_dev(c, sl.in, slab + 64)) != GCZ_OK) return r;
-    if ((r = ensure_dev(c, sv->wins[k], std::max<size_t>(nb, 1) * sizeof(gcz_window))) != GCZ_OK) return r;
-    uint8_t *slab_p = static_cast<uint8_t *>(sl.in.p);
-    for (ServerReq *q : b.reqs)
-        if (q->n) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + q->slab_off, q->src, q->n, cudaMemcpyHostToDevice, sl.st));
-    GCZ_CUDA(c, cudaMemcpyAsync(sv->wins[k].p, hw.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, sl.st));
-    const gcz::WinDesc *dw = static_cast<const gcz::WinDesc *>(sv->wins[k].p);
-    if (b.kind == 0) {
-        size_t cap = 0;
-        for (ServerReq *q : b.reqs) cap += gcz_zstd_max_sequences(q->n);
-        if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
-        if ((r = ensure_host(c, sl.h_off, (nb + 1) * 8)) != GCZ_OK) return r;
-        if ((r = zstd_device_core(c, sl.sc, slab_p, slab, b.depth, sl.seqs.p, cap, static_cast<uint64_t *>(sl.offsets.p),
-                                  sl.st, dw, nb)) != GCZ_OK)
-            return r;
-        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
-    } else if (b.kind == GCZ_REQ_ZSTD_FRAMES) {
-        // sequences, then the GPU entropy stage; only the frame offsets come back now
-        size_t cap = 0, fbound = 0;
-        for (ServerReq *q : b.reqs) {
-            cap += gcz_zstd_max_sequences(q->n);
-            fbound += gcz_zstd_frames_bound(q->n);
+    DeviceGuard dg(c->device);
+    uint32_t *status = static_cast<uint32_t *>(s.status.p);
+    uint8_t *slab_p = static_cast<uint8_t *>(s.in.p);
+    const gcz::WinDesc *dw = static_cast<const gcz::WinDesc *>(s.wins.p);
+    uint16_t *cand = static_cast<uint16_t *>(s.cand.p);
+    GCZ_CUDA(c, cudaMemsetAsync(status, 0, 8, s.st));  // this batch's error bits start clear
+    for (ServerReq *q : s.reqs)
+        if (q->selftest_iters) {  // a bounded wait that runs out: the batch must report GCZ_EDEVICE
+            selftest_wait_kernel<<<1, 32, 0, s.st>>>(status, q->selftest_iters);
+            GCZ_CUDA(c, cudaGetLastError());
         }
-        if ((r = ensure_dev(c, sl.offsets, (nb + 1) * 8)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, sl.seqs, std::max<size_t>(cap, 1) * 16)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, sl.frames, std::max<size_t>(fbound, 1))) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, sl.foff, (nb + 1) * 8)) != GCZ_OK) return r;
-        if ((r = ensure_host(c, sl.h_off, (nb + 1) * 8)) != GCZ_OK) return r;
-        uint64_t *d_off = static_cast<uint64_t *>(sl.offsets.p);
-        if ((r = zstd_device_core(c, sl.sc, slab_p, slab, b.depth, sl.seqs.p, cap, d_off, sl.st, dw, nb)) != GCZ_OK)
-            return r;
-        if ((r = zenc_core(c, sl.sc, slab_p, slab, sl.seqs.p, d_off, static_cast<uint8_t *>(sl.frames.p), fbound,
-                           static_cast<uint64_t *>(sl.foff.p), sl.st, dw, nb)) != GCZ_OK)
-            return r;
-        GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.foff.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
-    } else {
-        if ((r = ensure_dev(c, sl.lz_packed, slab * 4 + 64)) != GCZ_OK) return r;
-        if ((r = ensure_dev(c, sl.lz_has, nb + 16)) != GCZ_OK) return r;
+    for (ServerReq *q : s.reqs)
+        if (q->n) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + q->slab_off, q->src, q->n, cudaMemcpyHostToDevice, s.st));
+    if (nb) {
+        GCZ_CUDA(c, cudaMemcpyAsync(s.wins.p, s.hwins.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, s.st));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(slab_p, slab, kW, (uint32_t)nb, cand, c->num_sms, s.st, dw));
+    }
+    const uint32_t nz = s.wb[kGrpLzma];  // Zstd windows: sequences and frames groups
+    uint64_t *d_off = static_cast<uint64_t *>(s.offsets.p);
+    if (nz) {
+        uint32_t *counts = static_cast<uint32_t *>(s.counts.p);
+        for (int g = kGrpSeqLazy; g <= kGrpFramesGreedy; g++) {
+            const uint32_t a = s.wb[g], b = s.wb[g + 1];
+            if (a == b) continue;
+            gcz::Zstd2Launch l{};
+            l.src = slab_p;
+            l.cand = cand;
+            l.n = slab;
+            l.window = kW;
+            l.num_windows = b - a;
+            l.search_depth = (g == kGrpSeqLazy || g == kGrpFramesLazy) ? 16u : 1u;
+            l.max_seqs = kMaxSeqs;
+            l.seg = s.seg.p;  // groups run one after another on this stream
+            l.packed = static_cast<uint8_t *>(s.packed.p) + (size_t)a * kMaxSeqs * 8;
+            l.seq_counts = counts + a;
+            l.status = status;
+            l.num_sms = c->num_sms;
+            l.ctas_per_sm = c->parse_ctas;
+            l.wins = dw + a;
+            GCZ_CUDA(c, gcz::launch_zstd_parse(l, s.st));
+        }
+        GCZ_CUDA(c, gcz::launch_scan_counts(counts, nz, d_off, s.st));
+        GCZ_CUDA(c, gcz::launch_expand_seqs(s.packed.p, counts, d_off, nz, kMaxSeqs, s.seqs.p,
+                                            s.seqs.cap / 16, status, c->num_sms, s.st));
+        if (s.wb[kGrpFramesLazy])  // offsets of the sequences groups
+            GCZ_CUDA(c, cudaMemcpyAsync(s.h_off.p, d_off, (s.wb[kGrpFramesLazy] + 1) * 8, cudaMemcpyDeviceToHost,
+                                        s.st));
+    }
+    const uint32_t f0 = s.wb[kGrpFramesLazy], nf = nz - f0;
+    if (nf) {
+        gcz::ZencLaunch l{};
+        l.src = slab_p;
+        l.n = slab;
+        l.window = kW;
+        l.num_windows = nf;
+        l.seqs = s.seqs.p;
+        l.seq_offsets = d_off + f0;
+        l.slots = static_cast<uint8_t *>(s.zslots.p);
+        l.ovs = static_cast<uint32_t *>(s.zovs.p);
+        l.sec_off = static_cast<uint32_t *>(s.zaux.p);
+        l.fsize = l.sec_off + nf;
+        l.raw = reinterpret_cast<uint8_t *>(l.fsize + nf);
+        l.plan = static_cast<uint8_t *>(s.zplan.p);
+        l.hist = reinterpret_cast<uint32_t *>(l.plan + nf * (size_t)gcz::kZencPlanBytes);
+        l.status = status;
+        l.num_sms = c->num_sms;
+        l.wins = dw + f0;
+        uint64_t *d_foff = static_cast<uint64_t *>(s.foff.p);
+        GCZ_CUDA(c, gcz::launch_zenc(l, s.st));
+        GCZ_CUDA(c, gcz::launch_scan_counts(l.fsize, nf, d_foff, s.st));
+        GCZ_CUDA(c, gcz::launch_zenc_compact(l, d_foff, static_cast<uint8_t *>(s.frames.p), s.frames.cap, s.st));
+        GCZ_CUDA(c, cudaMemcpyAsync(s.h_foff.p, d_foff, (nf + 1) * 8, cudaMemcpyDeviceToHost, s.st));
+    }
+    const uint32_t l0 = s.wb[kGrpLzma], nl = (uint32_t)nb - l0;
+    if (nl) {
         gcz::LzmaLaunch l{};
         l.src = slab_p;
         l.n = slab;
         l.window = kW;
-        l.num_windows = (uint32_t)nb;
-        l.search_depth = b.depth;
+        l.num_windows = nl;
+        l.search_depth = GCZ_LZMA2_SEARCH_DEPTH;
         l.max_matches = GCZ_LZMA2_MAX_MATCHES;
-        l.packed = static_cast<uint32_t *>(sl.lz_packed.p);
-        l.has_matches = static_cast<uint8_t *>(sl.lz_has.p);
-        l.status = c->d_status;
+        l.packed = static_cast<uint32_t *>(s.lz_packed.p);  // indexed by slab offset
+        l.has_matches = static_cast<uint8_t *>(s.lz_has.p);  // indexed from this group's first window
+        l.status = status;
         l.num_sms = c->num_sms;
         l.staged = 1;
-        l.wins = dw;
-        if ((r = lzma_run(c, sl.sc, l, sl.st)) != GCZ_OK) return r;
-        for (ServerReq *q : b.reqs) {
-            if (!q->n) continue;
+        l.wins = dw + l0;
+        GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, s.st));
+        for (ServerReq *q : s.reqs) {
+            if (q->group != kGrpLzma || !q->n) continue;
             if (q->out_a)
-                GCZ_CUDA(c, cudaMemcpyAsync(q->out_a, static_cast<uint32_t *>(sl.lz_packed.p) + q->slab_off, q->n * 4,
-                                            cudaMemcpyDeviceToHost, sl.st));
+                GCZ_CUDA(c, cudaMemcpyAsync(q->out_a, static_cast<uint32_t *>(s.lz_packed.p) + q->slab_off, q->n * 4,
+                                            cudaMemcpyDeviceToHost, s.st));
             if (q->out_b)
-                GCZ_CUDA(c, cudaMemcpyAsync(q->out_b, static_cast<uint8_t *>(sl.lz_has.p) + q->w0, q->nw,
-                                            cudaMemcpyDeviceToHost, sl.st));
+                GCZ_CUDA(c, cudaMemcpyAsync(q->out_b, static_cast<uint8_t *>(s.lz_has.p) + (q->w0 - l0), q->nw,
+                                            cudaMemcpyDeviceToHost, s.st));
         }
     }
-    GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
+    GCZ_CUDA(c, cudaMemcpyAsync(s.h_status.p, status, 8, cudaMemcpyDeviceToHost, s.st));
+    GCZ_CUDA(c, cudaLaunchHostFunc(s.st, slot_signal, &s));
     return GCZ_OK;
 }
 
-// Second half of a batch: wait for it, copy out the Zstd sequences of every
-// request (their counts are known now), complete the requests.
-void server_finish(gcz_server *sv, int k) {
+// The batch's kernels are done: check its status, copy each Zstd request's
+// sequences and each frames request's frames out (their sizes are known now)
+// and queue the signal again, or, with nothing left to copy, complete it.
+// Returns true when the slot's batch is complete.
+bool server_results(gcz_server *sv, ServerSlot &s) {
     gcz_ctx *c = sv->c;
-    Batch &b = sv->batch[k];
-    Slot &sl = sv->slots[k];
-    int r = b.err;  // a launch that failed part-way completes its requests with its status
-    if (r != GCZ_OK) {
-        // Copies that the failed launch did queue end before the requests go back.
-        DeviceGuard g(c->device);
-        cudaStreamSynchronize(sl.st);
+    const uint32_t h = static_cast<const uint32_t *>(s.h_status.p)[0];
+    if (h & 2u) s.err = GCZ_ECAPACITY;
+    else if (h & 4u) s.err = GCZ_EINVAL;
+    else if (h) s.err = GCZ_EDEVICE;
+    if (s.err != GCZ_OK) return true;
+    DeviceGuard dg(c->device);
+    bool queued = false;
+    const uint64_t *ho = static_cast<const uint64_t *>(s.h_off.p);
+    const uint64_t *hf = static_cast<const uint64_t *>(s.h_foff.p);
+    const uint32_t f0 = s.wb[kGrpFramesLazy];
+    for (ServerReq *q : s.reqs) {
+        if (q->group == kGrpLzma) continue;
+        const bool frames = q->group == kGrpFramesLazy || q->group == kGrpFramesGreedy;
+        const uint64_t *o = frames ? hf + (q->w0 - f0) : ho + q->w0;
+        const uint64_t a = o[0], e = o[q->nw];
+        uint64_t *ob = static_cast<uint64_t *>(q->out_b);
+        if (ob) {
+            if (frames)
+                for (uint32_t i = 0; i < q->nw; i++) ob[i] = o[i + 1] - o[i];
+            else
+                for (uint32_t i = 0; i <= q->nw; i++) ob[i] = o[i] - a;
+        }
+        if (e - a > q->cap_a) {
+            q->fail = GCZ_ECAPACITY;
+            continue;
+        }
+        if (e == a) continue;
+        const cudaError_t ce =
+            frames ? cudaMemcpyAsync(q->out_a, static_cast<uint8_t *>(s.frames.p) + a, e - a, cudaMemcpyDeviceToHost,
+                                     s.st)
+                   : cudaMemcpyAsync(q->out_a, static_cast<gcz_zstd_sequence *>(s.seqs.p) + a, (e - a) * 16,
+                                     cudaMemcpyDeviceToHost, s.st);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            s.err = GCZ_ECUDA;
+            break;
+        }
+        queued = true;
+    }
+    if (s.err != GCZ_OK) {
+        cudaStreamSynchronize(s.st);  // copies already queued end before the requests go back
+        cudaGetLastError();
+        return true;
+    }
+    if (!queued) return true;
+    if (cudaLaunchHostFunc(s.st, slot_signal, &s) != cudaSuccess) {
+        cudaGetLastError();
+        cudaStreamSynchronize(s.st);
         cudaGetLastError();
     } else {
-        DeviceGuard g(c->device);
-        if (cudaEventSynchronize(sl.ev) != cudaSuccess) r = GCZ_ECUDA;
-        if (r == GCZ_OK && b.kind == 0) {
-            const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);
-            for (ServerReq *q : b.reqs) {
-                const uint64_t a = ho[q->w0], e = ho[q->w0 + q->nw];
-                uint64_t *ob = static_cast<uint64_t *>(q->out_b);
-                if (ob)
-                    for (uint32_t i = 0; i <= q->nw; i++) ob[i] = ho[q->w0 + i] - a;
-                if (e - a > q->cap_a) {
-                    q->fail = GCZ_ECAPACITY;
-                    continue;
-                }
-                if (e > a &&
-                    cudaMemcpyAsync(q->out_a, static_cast<gcz_zstd_sequence *>(sl.seqs.p) + a, (e - a) * 16,
-                                    cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
-                    r = GCZ_ECUDA;
-            }
-            if (cudaStreamSynchronize(sl.st) != cudaSuccess) r = GCZ_ECUDA;
-        } else if (r == GCZ_OK && b.kind == GCZ_REQ_ZSTD_FRAMES) {
-            const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);  // frame byte offsets
-            for (ServerReq *q : b.reqs) {
-                const uint64_t a = ho[q->w0], e = ho[q->w0 + q->nw];
-                uint64_t *ob = static_cast<uint64_t *>(q->out_b);
-                if (ob)
-                    for (uint32_t i = 0; i < q->nw; i++) ob[i] = ho[q->w0 + i + 1] - ho[q->w0 + i];
-                if (e - a > q->cap_a) {
-                    q->fail = GCZ_ECAPACITY;
-                    continue;
-                }
-                if (e > a && cudaMemcpyAsync(q->out_a, static_cast<uint8_t *>(sl.frames.p) + a, e - a,
-                                             cudaMemcpyDeviceToHost, sl.st) != cudaSuccess)
-                    r = GCZ_ECUDA;
-            }
-            if (cudaStreamSynchronize(sl.st) != cudaSuccess) r = GCZ_ECUDA;
-        }
-        uint32_t h = 0;
-        if (cudaMemcpy(&h, c->d_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess) r = GCZ_ECUDA;
-        if (r == GCZ_OK && h) r = GCZ_EDEVICE;
+        return false;
     }
+    return true;
+}
+
+// Complete a slot's requests with the batch status (or their own failure) and free the slot.
+void server_complete(gcz_server *sv, ServerSlot &s) {
     const double t = now_ms();
     std::lock_guard<std::mutex> lk(sv->mu);
-    for (ServerReq *q : b.reqs) {
-        if (q->status == 1) q->status = q->fail != GCZ_OK ? q->fail : r;
+    for (ServerReq *q : s.reqs) {
+        if (q->status == 1) q->status = q->fail != GCZ_OK ? q->fail : s.err;
         q->t_done = t;
         const double lat = q->t_done - q->t_submit;
         if (sv->lat_ms.size() < gcz_server::kLatWindow) {
@@ -1346,72 +1482,104 @@ void server_finish(gcz_server *sv, int k) {
         sv->completed++;
         sv->bytes_done += q->n;
     }
+    if (s.err != GCZ_OK) sv->worker_error = s.err;
     sv->batches++;
-    b.reqs.clear();
-    b.busy = false;
+    s.reqs.clear();
+    s.phase = 0;
+    s.signaled = false;
+    s.err = GCZ_OK;
     sv->cv_done.notify_all();
+    sv->cv_work.notify_one();
 }
 
+// The worker: completes batches as their signals arrive and, whenever a slot
+// is free and requests are pending, admits the oldest pending requests of any
+// kind into a new batch and launches it at once, so up to nslots batches run
+// on the GPU together.
 void server_loop(gcz_server *sv) {
-    int k = 0;
     for (;;) {
-        Batch &b = sv->batch[k];
-        Batch &other = sv->batch[k ^ 1];
+        std::vector<ServerSlot *> ready;
+        ServerSlot *launch = nullptr;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
-            if (sv->pending.empty() && !sv->stop && !other.busy)
-                sv->cv_work.wait(lk, [&] { return sv->stop || !sv->pending.empty(); });
-            if (sv->pending.empty() && sv->stop && !other.busy) break;
-            // Admit pending requests of the first request's kind (and Zstd lazy
-            // mode) while the batch stays within the byte and count limits.
-            // Bytes are counted as laid out in the slab, each request padded to
-            // whole 64 KiB windows: every device buffer of a batch then stays
-            // within the size of one max_batch_bytes batch, so a burst of small
-            // requests never regrows (cudaFree synchronises the device) and the
-            // HBM budget holds.
-            uint64_t bytes = 0;
-            for (auto it = sv->pending.begin(); it != sv->pending.end();) {
-                ServerReq *q = *it;
-                const uint64_t padded = nwin(q->n) * (uint64_t)kW;
-                const bool same = b.reqs.empty() ||
-                                  (q->kind == b.kind && (q->kind == GCZ_REQ_LZMA2 || (q->depth > 1) == (b.depth > 1)));
-                if (same && (b.reqs.empty() || (bytes + padded <= sv->max_batch_bytes &&
-                                                b.reqs.size() < sv->max_batch_requests))) {
-                    if (b.reqs.empty()) {
-                        b.kind = q->kind;
-                        b.depth = q->depth;
-                    }
-                    q->t_admit = now_ms();
-                    bytes += padded;
-                    b.reqs.push_back(q);
-                    it = sv->pending.erase(it);
-                } else {
-                    ++it;
+            auto free_slot = [&]() -> ServerSlot * {
+                for (int k = 0; k < sv->nslots; k++)
+                    if (sv->slots[k].phase == 0) return &sv->slots[k];
+                return nullptr;
+            };
+            auto in_flight = [&] {
+                int n = 0;
+                for (int k = 0; k < sv->nslots; k++) n += sv->slots[k].phase != 0;
+                return n;
+            };
+            auto any_signal = [&] {
+                for (int k = 0; k < sv->nslots; k++)
+                    if (sv->slots[k].signaled) return true;
+                return false;
+            };
+            sv->cv_work.wait(lk, [&] {
+                return any_signal() || (!sv->pending.empty() && free_slot()) ||
+                       (sv->stop && sv->pending.empty() && in_flight() == 0);
+            });
+            if (sv->stop && sv->pending.empty() && in_flight() == 0) break;
+            for (int k = 0; k < sv->nslots; k++)
+                if (sv->slots[k].signaled) {
+                    sv->slots[k].signaled = false;
+                    ready.push_back(&sv->slots[k]);
                 }
+            ServerSlot *fs = sv->pending.empty() ? nullptr : free_slot();
+            if (fs) {
+                // Requests are counted in whole 64 KiB windows, as they are
+                // laid out in the slab, so a batch never needs more than the
+                // slot's pre-sized buffers.  The oldest request always fits.
+                uint64_t bytes = 0;
+                const double t = now_ms();
+                for (auto it = sv->pending.begin(); it != sv->pending.end();) {
+                    ServerReq *q = *it;
+                    const uint64_t padded = nwin(q->n) * (uint64_t)kW;
+                    if (fs->reqs.empty() ||
+                        (bytes + padded <= sv->max_batch_bytes && fs->reqs.size() < sv->max_batch_requests)) {
+                        q->t_admit = t;
+                        q->group = req_group(q);
+                        bytes += padded;
+                        fs->reqs.push_back(q);
+                        it = sv->pending.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+                fs->phase = 1;
+                fs->err = GCZ_OK;
+                launch = fs;
+                sv->max_in_flight = std::max<uint64_t>(sv->max_in_flight, (uint64_t)in_flight());
             }
         }
-        if (!b.reqs.empty()) {
-            // A failed launch is recorded on the batch; server_finish completes
-            // its requests.  Setting their status here would let a waiter free
-            // a request the batch still holds.
+        for (ServerSlot *s : ready) {
+            bool done = true;
+            if (s->phase == 1) {
+                s->phase = 2;
+                done = server_results(sv, *s);
+            }
+            if (done) server_complete(sv, *s);
+        }
+        if (launch) {
             int r;
             try {
-                r = server_launch(sv, k);
+                r = server_launch(sv, *launch);
             } catch (const std::exception &) {  // host memory: never let it end the worker thread
                 r = GCZ_ENOMEM;
             }
-            b.err = r;
-            b.busy = true;
             if (r != GCZ_OK) {
-                std::lock_guard<std::mutex> lk(sv->mu);
-                sv->worker_error = r;
+                // Nothing signals a batch whose launch failed part-way: drain
+                // what it did queue, then complete its requests with the status.
+                DeviceGuard dg(sv->c->device);
+                cudaStreamSynchronize(launch->st);
+                cudaGetLastError();
+                launch->err = r;
+                server_complete(sv, *launch);
             }
         }
-        if (other.busy) server_finish(sv, k ^ 1);  // overlaps with batch k on the GPU
-        if (!b.reqs.empty()) k ^= 1;
     }
-    for (int j = 0; j < 2; j++)
-        if (sv->batch[j].busy) server_finish(sv, j);
 }
 
 }  // namespace
@@ -1420,40 +1588,53 @@ extern "C" int gcz_server_create(gcz_ctx *c, uint64_t hbm_budget, uint64_t max_b
                                  uint32_t max_batch_requests, gcz_server **out) {
     if (!c || !out) return GCZ_EINVAL;
     *out = nullptr;
+    // Slot count and batch size from the budget: each slot holds ~22 device
+    // bytes per input byte of a max-size batch.  With no batch size given, the
+    // budget is split over four slots.
+    const uint64_t per_byte_budget = (uint64_t)(hbm_budget / kDeviceBytesPerInputByte);
+    if (max_batch_bytes == 0) max_batch_bytes = per_byte_budget / 4;
+    max_batch_bytes = std::min<uint64_t>(max_batch_bytes, per_byte_budget) & ~uint64_t(kW - 1);
+    if (max_batch_bytes < kW) return fail(c, GCZ_EINVAL, "HBM budget too small for one 64 KiB window per batch");
+    const int nslots = (int)std::max<uint64_t>(1, std::min<uint64_t>(kMaxServerSlots, per_byte_budget / max_batch_bytes));
     gcz_server *sv = new (std::nothrow) gcz_server();
     if (!sv) return fail(c, GCZ_ENOMEM, "server allocation failed");
     sv->c = c;
-    // Failure after this point: release the streams and events made so far.
-    auto release = [&] {
-        DeviceGuard g(c->device);
-        for (Slot &sl : sv->slots) {
-            if (sl.ev) cudaEventDestroy(sl.ev);
-            if (sl.st) cudaStreamDestroy(sl.st);
-        }
-        delete sv;
-    };
-    uint64_t cap = (uint64_t)(hbm_budget / (2.0 * kDeviceBytesPerInputByte));
-    if (max_batch_bytes == 0 || max_batch_bytes > cap) max_batch_bytes = cap;
-    sv->max_batch_bytes = max_batch_bytes & ~uint64_t(kW - 1);
-    if (sv->max_batch_bytes < kW) {
-        delete sv;
-        return fail(c, GCZ_EINVAL, "HBM budget too small for one 64 KiB window per batch");
-    }
+    sv->max_batch_bytes = max_batch_bytes;
     sv->max_batch_requests = max_batch_requests ? max_batch_requests : 65536;
+    sv->nslots = nslots;
+    int r = GCZ_OK;
     {
         DeviceGuard g(c->device);
-        for (Slot &sl : sv->slots)
-            if (cudaStreamCreateWithFlags(&sl.st, cudaStreamNonBlocking) != cudaSuccess ||
-                cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
+        for (int k = 0; k < nslots && r == GCZ_OK; k++) {
+            ServerSlot &s = sv->slots[k];
+            s.sv = sv;
+            s.index = k;
+            if (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess) {
                 cudaGetLastError();
-                release();
-                return GCZ_ECUDA;
+                r = fail(c, GCZ_ECUDA, "server stream creation failed");
+                break;
             }
+            r = slot_alloc(c, s, max_batch_bytes);
+        }
+        if (r != GCZ_OK) {
+            for (int k = 0; k < nslots; k++) slot_release(sv->slots[k]);
+            delete sv;
+            return r;
+        }
+        for (int k = 0; k < nslots; k++)
+            for (DevBuf *b : {&sv->slots[k].in, &sv->slots[k].wins, &sv->slots[k].status, &sv->slots[k].cand,
+                              &sv->slots[k].seg, &sv->slots[k].packed, &sv->slots[k].counts, &sv->slots[k].offsets,
+                              &sv->slots[k].seqs, &sv->slots[k].lz_packed, &sv->slots[k].lz_has,
+                              &sv->slots[k].frames, &sv->slots[k].foff, &sv->slots[k].zslots, &sv->slots[k].zovs,
+                              &sv->slots[k].zaux, &sv->slots[k].zplan})
+                sv->device_bytes += b->cap;
     }
     try {
         sv->worker = std::thread(server_loop, sv);
     } catch (const std::exception &) {  // a thread limit: report it, never throw through the C ABI
-        release();
+        DeviceGuard g(c->device);
+        for (int k = 0; k < nslots; k++) slot_release(sv->slots[k]);
+        delete sv;
         return fail(c, GCZ_ENOMEM, "could not start the request loop's worker thread");
     }
     *out = sv;
@@ -1470,16 +1651,7 @@ extern "C" void gcz_server_destroy(gcz_server *sv) {
     if (sv->worker.joinable()) sv->worker.join();
     {
         DeviceGuard g(sv->c->device);
-        for (int j = 0; j < 2; j++) {
-            Slot &sl = sv->slots[j];
-            for (DevBuf *b : {&sl.sc.packed, &sl.sc.counts, &sl.sc.cand, &sl.sc.seg, &sl.sc.zslots, &sl.sc.zovs,
-                              &sl.sc.zaux, &sl.sc.zplan, &sl.in, &sl.offsets, &sl.seqs, &sl.lz_packed, &sl.lz_has,
-                              &sl.frames, &sl.foff, &sv->wins[j]})
-                if (b->p) cudaFree(b->p);
-            if (sl.h_off.p) cudaFreeHost(sl.h_off.p);
-            if (sl.ev) cudaEventDestroy(sl.ev);
-            if (sl.st) cudaStreamDestroy(sl.st);
-        }
+        for (int k = 0; k < sv->nslots; k++) slot_release(sv->slots[k]);
     }
     for (auto &kv : sv->reqs) delete kv.second;
     delete sv;
@@ -1487,13 +1659,20 @@ extern "C" void gcz_server_destroy(gcz_server *sv) {
 
 extern "C" uint64_t gcz_server_max_batch_bytes(const gcz_server *sv) { return sv ? sv->max_batch_bytes : 0; }
 
+extern "C" int gcz_server_info(const gcz_server *sv, uint32_t *slots, uint64_t *device_bytes) {
+    if (!sv) return GCZ_EINVAL;
+    if (slots) *slots = (uint32_t)sv->nslots;
+    if (device_bytes) *device_bytes = sv->device_bytes;
+    return GCZ_OK;
+}
+
 extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth, const uint8_t *src, size_t n,
                                  void *out_a, size_t cap_a, void *out_b, uint64_t *id) {
     if (!sv || !id || (kind != GCZ_REQ_ZSTD && kind != GCZ_REQ_LZMA2 && kind != GCZ_REQ_ZSTD_FRAMES) || (n && !src))
         return GCZ_EINVAL;
     if (kind == GCZ_REQ_ZSTD && (!out_b || (n && !out_a))) return GCZ_EINVAL;
     if (kind == GCZ_REQ_ZSTD_FRAMES && n && (!out_a || !out_b)) return GCZ_EINVAL;
-    if (n > sv->max_batch_bytes) return GCZ_ETOOLARGE;
+    if (nwin(n) * (uint64_t)kW > sv->max_batch_bytes) return GCZ_ETOOLARGE;
     ServerReq *q = new (std::nothrow) ServerReq();
     if (!q) return GCZ_ENOMEM;
     q->kind = kind;
@@ -1521,6 +1700,30 @@ extern "C" int gcz_server_submit(gcz_server *sv, int kind, uint32_t search_depth
     return GCZ_OK;
 }
 
+extern "C" int gcz_server_selftest_wait_timeout(gcz_server *sv, uint32_t max_iterations, uint64_t *id) {
+    if (!sv || !id || max_iterations == 0) return GCZ_EINVAL;
+    ServerReq *q = new (std::nothrow) ServerReq();
+    if (!q) return GCZ_ENOMEM;
+    q->kind = GCZ_REQ_LZMA2;  // no windows: it joins a batch like any request
+    q->selftest_iters = max_iterations;
+    q->t_submit = now_ms();
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        q->id = sv->next_id++;
+        try {
+            sv->reqs[q->id] = q;
+            sv->pending.push_back(q);
+        } catch (const std::exception &) {
+            sv->reqs.erase(q->id);
+            delete q;
+            return GCZ_ENOMEM;
+        }
+        *id = q->id;
+    }
+    sv->cv_work.notify_one();
+    return GCZ_OK;
+}
+
 extern "C" int gcz_server_wait(gcz_server *sv, uint64_t id, double timeout_s, double *latency_ms) {
     if (!sv) return GCZ_EINVAL;
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -1535,7 +1738,7 @@ extern "C" int gcz_server_wait(gcz_server *sv, uint64_t id, double timeout_s, do
     const bool ok =
         sv->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return gone() || q->status != 1; });
     if (gone()) return GCZ_EINVAL;
-    if (!ok) return GCZ_EDEVICE;
+    if (!ok) return GCZ_ETIMEOUT;  // still queued or running: its buffers stay in use
     const int st = q->status;
     if (latency_ms) *latency_ms = q->t_done - q->t_submit;
     sv->reqs.erase(id);

@@ -22,10 +22,14 @@
 //    workload a guessed parse meets the true one after ~180 bytes, three
 //    matches, so the overlap costs ~4% extra parse work.)
 //    Each warp parses like the reference, one match at a time, but with all
-//    32 lanes: the hash-match bits of the next 32 positions come from the
-//    bitmap, the lanes test the three repeat offsets (:259-275) on their own
-//    positions, a ballot finds the first event, matches are extended 128
-//    bytes per warp iteration, and one lazy step (:278-307) follows.
+//    32 lanes: the hash-match bits of the next positions come from the
+//    bitmap, the lanes test the three repeat offsets (:259-275) on the
+//    positions before the first hash match -- one (position, offset) pair per
+//    lane when there are at most 10 of them, one position per lane up to 32,
+//    and four positions per lane (8-byte compares) over up to 128 positions
+//    that hold no hash match -- a ballot finds the first event, matches are
+//    extended 128 bytes per warp iteration, and one lazy step (:278-307)
+//    follows.
 // 3. The chain is written as packed {ll | (ml-3) << 16, off} (or the
 //    reference's {ll, ml-3, off} triples) at the per-window stride, capped at
 //    max_seqs exactly like the reference's `num_seqs < max_sequences_per_chunk`
@@ -45,9 +49,10 @@ constexpr uint32_t kMinMatch = 3;                 // MIN_MATCH_LEN, zstd_compres
 constexpr uint32_t kSegW = 4096;                  // bytes per speculative segment (one warp)
 constexpr uint32_t kWarps = kMaxWindow / kSegW;   // 16 segments per full window
 constexpr uint32_t kThreads = kWarps * 32;
-// A warp's own parse starts matches in [seg_start, seg_end + 32) (its last
-// step looks up to 31 positions ahead, the lazy step one more) and matches
-// are >= 3 bytes; lists are written in 32-entry blocks.
+// A warp's own parse ends with a step that starts before seg_end and looks at
+// most 127 positions ahead (a wide scan), the lazy step one more; matches do not
+// overlap and are >= 3 bytes, so a list holds at most (kSegW - 1) / 3 + 1
+// entries; lists are written in 32-entry blocks.
 constexpr uint32_t kSpecCap = ((kSegW + 33) / 3 + 1 + 31) / 32 * 32;  // 1408
 constexpr uint32_t kContCap = 256;               // continuation matches before giving up
 constexpr uint32_t kLaneCap = kSpecCap + kContCap;
@@ -55,7 +60,7 @@ constexpr uint32_t kNoWarp = 0xFFFFu;
 
 constexpr uint32_t kPre = 64;                           // zero bytes before the window
 constexpr uint32_t kDataBytes = kPre + kMaxWindow + 64; // + zero pad after it
-constexpr uint32_t kBmWords = kMaxWindow / 32 + 2;
+constexpr uint32_t kBmWords = kMaxWindow / 32 + 8;  // the wide scan reads up to 4 words past a step's first
 
 struct SmemLayout {
     uint8_t data[kDataBytes];
@@ -228,35 +233,110 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, Cand
     if (nscan < 32u) H &= (1u << nscan) - 1u;
     const uint32_t q = p + lane;
     cb.advance(p);  // candidates of p .. p+32 (and the next block in flight)
-    uint32_t f, rsel = 0;
+    uint32_t f, r = 0;  // event position; for a repeat-offset match, which repeat offset (0-2)
     bool hash;
     if (H & 1u) {
         f = p;
         hash = true;
     } else {
+        // Repeat offsets are tried only at positions without a hash match, in
+        // order r0, r1, r2, and the first position with a hit wins
+        // (zstd_compress.cu:259-275).  How the lanes share the tests depends
+        // on how many positions come before the first hash match.
         const uint32_t n = H ? static_cast<uint32_t>(__ffs(H)) - 1u : nscan;  // positions without a hash match
-        const bool need = lane < n;
-        const uint32_t x = w.u32(static_cast<int>(q));
-        const bool a0 =
-            need && s.r0 <= q && ((x ^ w.u32(static_cast<int>(s.r0 <= q ? q - s.r0 : 0u))) & 0xFFFFFFu) == 0u;
-        const bool a1 = need && !a0 && s.r1 <= q &&
-                        ((x ^ w.u32(static_cast<int>(s.r1 <= q ? q - s.r1 : 0u))) & 0xFFFFFFu) == 0u;
-        const bool a2 = need && !a0 && !a1 && s.r2 <= q &&
-                        ((x ^ w.u32(static_cast<int>(s.r2 <= q ? q - s.r2 : 0u))) & 0xFFFFFFu) == 0u;
-        rsel = a0 ? 0u : (a1 ? 1u : 2u);
-        const uint32_t rb = __ballot_sync(kFull, a0 || a1 || a2);
-        if (rb) {
-            f = p + static_cast<uint32_t>(__ffs(rb)) - 1u;
-            hash = false;
-        } else if (H) {
-            f = p + n;
-            hash = true;
+        if (n <= 10u) {
+            // Few positions: one (position, repeat offset) pair per lane, in
+            // position-major order, so the first set ballot bit is the event.
+            const uint32_t i = lane / 3u, k = lane - 3u * i;
+            const uint32_t rv = k == 0u ? s.r0 : (k == 1u ? s.r1 : s.r2);
+            const uint32_t qq = p + i;
+            const bool hit = i < n && rv <= qq && eq3(w, qq, rv <= qq ? qq - rv : qq);
+            const uint32_t rb = __ballot_sync(kFull, hit);
+            if (rb) {
+                const uint32_t l = static_cast<uint32_t>(__ffs(rb)) - 1u;
+                f = p + l / 3u;
+                r = l % 3u;
+                hash = false;
+            } else if (H) {
+                f = p + n;
+                hash = true;
+            } else {
+                s.p = p + nscan;
+                return false;
+            }
+        } else if (H == 0u && lim > 32u) {
+            // No hash match in 32 positions: scan up to 128, four positions
+            // per lane, each repeat offset tested on 8-byte words.
+            const uint32_t n4s = lim < 128u ? lim : 128u;
+            const uint32_t wi = p >> 5, sh = p & 31u;
+            uint32_t n4 = n4s;
+#pragma unroll
+            for (uint32_t k = 3; k >= 1; --k) {
+                const uint32_t hk = __funnelshift_r(bm[wi + k], bm[wi + k + 1u], sh);
+                if (hk) n4 = 32u * k + static_cast<uint32_t>(__ffs(hk)) - 1u;
+            }
+            if (n4 > n4s) n4 = n4s;
+            const uint32_t j0 = 4u * lane;  // this lane's first position index
+            const uint32_t q0 = j0 < n4 ? p + j0 : p;
+            const uint32_t vlim = j0 < n4 ? (n4 - j0 < 4u ? n4 - j0 : 4u) : 0u;  // positions of this lane to test
+            const uint32_t xlo = w.u32(static_cast<int>(q0)), xhi = w.u32(static_cast<int>(q0 + 4u));
+            uint32_t mk[3];
+#pragma unroll
+            for (uint32_t k = 0; k < 3; ++k) {
+                const uint32_t rv = k == 0u ? s.r0 : (k == 1u ? s.r1 : s.r2);
+                // positions q0 + t with t < vlim and q0 + t >= rv; their source bytes start at q0 - rv + t >= 0
+                const uint32_t tmin = rv > q0 ? rv - q0 : 0u;
+                uint32_t valid = tmin < vlim ? ((1u << vlim) - 1u) & ~((1u << tmin) - 1u) : 0u;
+                const int yb = valid ? static_cast<int>(q0) - static_cast<int>(rv) : static_cast<int>(q0);
+                const uint32_t dlo = xlo ^ w.u32(yb), dhi = xhi ^ w.u32(yb + 4);
+                const uint32_t e = ((dlo & 0xFFFFFFu) == 0u ? 1u : 0u) | ((dlo >> 8) == 0u ? 2u : 0u) |
+                                   ((__funnelshift_r(dlo, dhi, 16) & 0xFFFFFFu) == 0u ? 4u : 0u) |
+                                   ((__funnelshift_r(dlo, dhi, 24) & 0xFFFFFFu) == 0u ? 8u : 0u);
+                mk[k] = e & valid;
+            }
+            const uint32_t any = mk[0] | mk[1] | mk[2];
+            const uint32_t rb = __ballot_sync(kFull, any != 0u);
+            if (rb) {
+                const uint32_t l = static_cast<uint32_t>(__ffs(rb)) - 1u;
+                const uint32_t al = __shfl_sync(kFull, any, l), m0 = __shfl_sync(kFull, mk[0], l),
+                               m1 = __shfl_sync(kFull, mk[1], l);
+                const uint32_t t = static_cast<uint32_t>(__ffs(al)) - 1u;
+                f = p + 4u * l + t;
+                r = (m0 >> t) & 1u ? 0u : ((m1 >> t) & 1u ? 1u : 2u);
+                hash = false;
+            } else if (n4 < n4s) {
+                f = p + n4;
+                hash = true;
+            } else {
+                s.p = p + n4s;
+                return false;
+            }
         } else {
-            s.p = p + nscan;
-            return false;
+            const bool need = lane < n;
+            const uint32_t x = w.u32(static_cast<int>(q));
+            const bool a0 =
+                need && s.r0 <= q && ((x ^ w.u32(static_cast<int>(s.r0 <= q ? q - s.r0 : 0u))) & 0xFFFFFFu) == 0u;
+            const bool a1 = need && !a0 && s.r1 <= q &&
+                            ((x ^ w.u32(static_cast<int>(s.r1 <= q ? q - s.r1 : 0u))) & 0xFFFFFFu) == 0u;
+            const bool a2 = need && !a0 && !a1 && s.r2 <= q &&
+                            ((x ^ w.u32(static_cast<int>(s.r2 <= q ? q - s.r2 : 0u))) & 0xFFFFFFu) == 0u;
+            const uint32_t rsel = a0 ? 0u : (a1 ? 1u : 2u);
+            const uint32_t rb = __ballot_sync(kFull, a0 || a1 || a2);
+            if (rb) {
+                const uint32_t l = static_cast<uint32_t>(__ffs(rb)) - 1u;
+                f = p + l;
+                r = __shfl_sync(kFull, rsel, l);
+                hash = false;
+            } else if (H) {
+                f = p + n;
+                hash = true;
+            } else {
+                s.p = p + nscan;
+                return false;
+            }
         }
     }
-    const uint32_t fi = f - p;
+    cb.advance(f);  // a wide scan's event can lie past the buffer
     const uint32_t cf = zmap(cb.get(f));
     const uint32_t cf1 = zmap(cb.get(f + 1u));
     uint32_t off, c0;
@@ -264,7 +344,6 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, Cand
         off = f - cf;
         c0 = cf;
     } else {  // first repeat offset with 3 equal bytes wins
-        const uint32_t r = __shfl_sync(kFull, rsel, fi);
         off = r == 0u ? s.r0 : (r == 1u ? s.r1 : s.r2);
         c0 = f - off;
     }

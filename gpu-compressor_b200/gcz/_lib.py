@@ -16,6 +16,9 @@ GCZ_ENOMEM = -3
 GCZ_ECAPACITY = -4
 GCZ_EDEVICE = -5
 GCZ_ETOOLARGE = -6
+GCZ_EUNAVAILABLE = -7
+GCZ_ECODEC = -8
+GCZ_ETIMEOUT = -9
 NOALLOC_MAX_INPUT = 8 << 20
 
 WINDOW = 65536
@@ -54,6 +57,8 @@ SIGNATURES = {
     "gcz_server_create": (_i, [_vp, _u64, _u64, _u32, ctypes.POINTER(_vp)]),
     "gcz_server_destroy": (None, [_vp]),
     "gcz_server_max_batch_bytes": (_u64, [_vp]),
+    "gcz_server_info": (_i, [_vp, ctypes.POINTER(_u32), ctypes.POINTER(_u64)]),
+    "gcz_server_selftest_wait_timeout": (_i, [_vp, _u32, ctypes.POINTER(_u64)]),
     "gcz_server_submit": (_i, [_vp, _i, _u32, _vp, _sz, _vp, _sz, _vp, ctypes.POINTER(_u64)]),
     "gcz_server_wait": (_i, [_vp, _u64, _d, ctypes.POINTER(_d)]),
     "gcz_server_stats": (_i, [_vp, ctypes.POINTER(_u64), ctypes.POINTER(_u64), ctypes.POINTER(_u64),

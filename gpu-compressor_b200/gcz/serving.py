@@ -5,6 +5,7 @@ import threading
 import numpy as np
 
 from . import L, GczError, num_windows, _u8
+from ._lib import GCZ_ETIMEOUT
 
 ZSTD, LZMA2, ZSTD_FRAMES = 0, 1, 2
 
@@ -61,6 +62,7 @@ class Server:
             raise GczError(rc, L.gcz_last_error(ctx.handle).decode(errors="replace"))
         self._h = h
         self._lock = threading.Lock()
+        self._live = {}  # id -> Request until a wait collects it: its buffers are in use until then
         self.ctx = ctx
         self._lib = L  # kept for close() during interpreter shutdown
 
@@ -68,10 +70,18 @@ class Server:
     def max_batch_bytes(self):
         return int(L.gcz_server_max_batch_bytes(self._h))
 
+    def info(self):
+        """(slots, device bytes held): every slot's buffers are allocated at creation."""
+        slots, dev = ctypes.c_uint32(), ctypes.c_uint64()
+        rc = L.gcz_server_info(self._h, ctypes.byref(slots), ctypes.byref(dev))
+        if rc != 0:
+            raise GczError(rc, "gcz_server_info failed")
+        return slots.value, dev.value
+
     def warm_up(self, kinds=(ZSTD, LZMA2)):
-        """Grow both slots' device buffers to a full batch of each kind before
-        latency-sensitive traffic: two max-size requests per kind, back to
-        back, because the worker alternates slots on every batch.  The device
+        """One max-size request of each kind, so that the first requests that
+        matter do not pay for first-launch costs (module loading, shared-memory
+        carve-out).  Device buffers are allocated at creation already.  The
         buffers are sized from byte and window counts, not from the content, so
         zero bytes do (with small host outputs: zero windows give one sequence,
         or one tiny frame, each)."""
@@ -79,14 +89,13 @@ class Server:
         nb = num_windows(n)
         data = np.zeros(n, np.uint8)
         for kind in kinds:
-            for _ in range(2):
-                if kind == ZSTD:
-                    r = self.submit(kind, data, out_a=np.empty((4 * nb, 4), np.uint32), cap=4 * nb)
-                elif kind == ZSTD_FRAMES:
-                    r = self.submit(kind, data, out_a=np.empty(64 * nb, np.uint8), cap=64 * nb)
-                else:
-                    r = self.submit(kind, data, packed=False)
-                self.wait(r)
+            if kind == ZSTD:
+                r = self.submit(kind, data, out_a=np.empty((4 * nb, 4), np.uint32), cap=4 * nb)
+            elif kind == ZSTD_FRAMES:
+                r = self.submit(kind, data, out_a=np.empty(64 * nb, np.uint8), cap=64 * nb)
+            else:
+                r = self.submit(kind, data, packed=False)
+            self.wait(r)
 
     def submit(self, kind, data, depth=None, **outputs):
         depth = (32 if kind == LZMA2 else 16) if depth is None else depth
@@ -98,11 +107,32 @@ class Server:
         if rc != 0:
             raise GczError(rc, "gcz_server_submit failed")
         r.id = rid.value
+        with self._lock:
+            self._live[r.id] = r
+        return r
+
+    def selftest_wait_timeout(self, max_iterations=1 << 12):
+        """Submit a failure-detection probe (gcz_server_selftest_wait_timeout):
+        its batch's bounded wait runs out and the batch reports GCZ_EDEVICE."""
+        r = Request(LZMA2, np.zeros(0, np.uint8), 32, packed=False)
+        rid = ctypes.c_uint64()
+        rc = L.gcz_server_selftest_wait_timeout(self._h, int(max_iterations), ctypes.byref(rid))
+        if rc != 0:
+            raise GczError(rc, "gcz_server_selftest_wait_timeout failed")
+        r.id = rid.value
+        with self._lock:
+            self._live[r.id] = r
         return r
 
     def wait(self, r, timeout_s=600.0):
+        """The request's result.  GczError with code GCZ_ETIMEOUT when timeout_s
+        passed first: the request stays in the loop, and the server keeps its
+        buffers alive until a later wait collects it."""
         lat = ctypes.c_double()
         rc = L.gcz_server_wait(self._h, r.id, float(timeout_s), ctypes.byref(lat))
+        if rc != GCZ_ETIMEOUT:
+            with self._lock:
+                self._live.pop(r.id, None)
         if rc != 0:
             raise GczError(rc, f"request {r.id} failed")
         r.latency_ms = lat.value
@@ -118,8 +148,9 @@ class Server:
 
     def close(self):
         if getattr(self, "_h", None):
-            self._lib.gcz_server_destroy(self._h)
+            self._lib.gcz_server_destroy(self._h)  # finishes every submitted request first
             self._h = None
+            self._live = {}
 
     def __del__(self):
         self.close()

@@ -43,6 +43,7 @@ enum {
     GCZ_ETOOLARGE = -6,  /* input larger than gcz_zstd_match_find_device_noalloc's static scratch */
     GCZ_EUNAVAILABLE = -7, /* a run-time library the call needs (libzstd) could not be loaded */
     GCZ_ECODEC = -8,     /* the CPU entropy coder failed */
+    GCZ_ETIMEOUT = -9,   /* gcz_server_wait gave up; the request is still queued or running */
 };
 
 typedef struct gcz_ctx gcz_ctx;
@@ -230,21 +231,25 @@ int gcz_zstd_match_find_files(gcz_ctx *ctx, const uint8_t *const *srcs, const si
 
 /* ---------------------------------------------------------------- serving */
 
-/* A request loop over one context: requests of mixed kind and size are
- * submitted at any time and admitted into the next batch while its input,
- * each request counted in whole 64 KiB windows as it is laid out on the
- * device, stays within max_batch_bytes (derived from hbm_budget: two batches
- * are in flight, each needing at most ~18 device bytes per input byte).  So no
- * batch needs more device memory than one max_batch_bytes batch, and once the
- * buffers have grown to that (a first large batch), none regrows.  One worker thread
- * launches a batch on one stream while it completes the previous batch on the
- * other, so requests that arrive while a batch runs join the next one.  Every
- * request gets exactly the result it would get alone (windows are independent).
- * src and the output buffers must stay valid until gcz_server_wait returns.
- * The first batch of a kind on each of the two slots allocates that kind's
- * device buffers (cudaMalloc; cudaFree before a regrowth waits for the
- * device): two max-size requests of each kind, back to back, warm both slots
- * before traffic whose latency matters. */
+/* A request loop over one context (continuous batching).  Requests of any
+ * kind and size are submitted at any time.  The loop keeps up to 8 slots, each
+ * a stream with every device buffer a batch of max_batch_bytes needs, of any mix
+ * of kinds, allocated once by gcz_server_create (~22 device bytes per input
+ * byte per slot; the slot count is hbm_budget / (22 * max_batch_bytes), at
+ * most 8, so the budget holds and serving never calls cudaMalloc or cudaFree).
+ * Whenever a slot is free and requests are pending, one worker thread admits
+ * the oldest pending requests -- Zstd sequences, Zstd frames and LZMA2
+ * together, each counted in whole 64 KiB windows as it is laid out on the
+ * device -- into a batch of at most max_batch_bytes and launches it at once:
+ * one candidate sweep over all its windows, then each kind's second stage.
+ * Batches on different slots run on the GPU at the same time; a batch's
+ * results are copied out as soon as its kernels finish (a host callback wakes
+ * the worker).  Every request gets exactly the result it would get alone
+ * (windows are independent).  src and the output buffers must stay valid until
+ * gcz_server_wait returns the request's own status (not GCZ_ETIMEOUT), or until
+ * gcz_server_destroy returns.  max_batch_bytes = 0 splits the budget over four
+ * slots.  Each batch has its own device status words, cleared at its launch, so
+ * an error affects only the batch that hit it. */
 typedef struct gcz_server gcz_server;
 enum { GCZ_REQ_ZSTD = 0, GCZ_REQ_LZMA2 = 1, GCZ_REQ_ZSTD_FRAMES = 2 };
 
@@ -252,18 +257,30 @@ int gcz_server_create(gcz_ctx *ctx, uint64_t hbm_budget, uint64_t max_batch_byte
                       gcz_server **out);
 void gcz_server_destroy(gcz_server *server);  /* finishes every submitted request first */
 uint64_t gcz_server_max_batch_bytes(const gcz_server *server);
+/* Slots (batches that can be on the GPU at once) and device bytes the loop holds. */
+int gcz_server_info(const gcz_server *server, uint32_t *slots, uint64_t *device_bytes);
 /* GCZ_REQ_ZSTD: out_a = gcz_zstd_sequence[cap_a], out_b = uint64_t[num_windows+1] offsets.
  * GCZ_REQ_LZMA2: out_a = uint32_t[n] packed (or NULL), out_b = uint8_t[num_windows] has-match bytes
  * (or NULL).  GCZ_REQ_ZSTD_FRAMES: the GPU frames of gcz_zstd_compress_frames_gpu -- out_a =
  * uint8_t[cap_a] frames back to back (gcz_zstd_frames_bound(n) always suffices), out_b =
  * uint64_t[num_windows] frame sizes.  search_depth as for the direct calls.  GCZ_ETOOLARGE if
- * n > max batch bytes.  The HBM budget allows ~18 device bytes per input byte of a batch. */
+ * n > max batch bytes. */
 int gcz_server_submit(gcz_server *server, int kind, uint32_t search_depth, const uint8_t *src, size_t n, void *out_a,
                       size_t cap_a, void *out_b, uint64_t *request_id);
-/* Blocks until the request is done (or timeout_s passes: GCZ_EDEVICE) and returns its
- * status; latency_ms = submit-to-completion time.  Each request is collected by
- * one wait: GCZ_EINVAL for an unknown id or one already collected. */
+/* Blocks until the request is done and returns its status; latency_ms =
+ * submit-to-completion time.  Each request is collected by one wait: GCZ_EINVAL
+ * for an unknown id or one already collected.  When timeout_s passes first the
+ * call returns GCZ_ETIMEOUT and the request stays in the loop (queued or
+ * running): its input and output buffers are still in use until a later wait
+ * collects it or gcz_server_destroy returns. */
 int gcz_server_wait(gcz_server *server, uint64_t request_id, double timeout_s, double *latency_ms);
+/* Failure detection without a GPU fault: submits a request whose batch runs
+ * one CTA that waits on an mbarrier nothing completes, with the same kind of
+ * bounded wait the kernels use (max_iterations tries).  The wait runs out, the
+ * kernel records it in that batch's status word and returns; waiting on the
+ * id gives GCZ_EDEVICE, for every request of that batch, while batches before
+ * and after it complete normally. */
+int gcz_server_selftest_wait_timeout(gcz_server *server, uint32_t max_iterations, uint64_t *request_id);
 /* Completed requests, their input bytes, batches launched, and the p50/p99 of
  * submit-to-completion latency (ms) over the most recent 2^20 completed requests. */
 int gcz_server_stats(gcz_server *server, uint64_t *completed, uint64_t *bytes, uint64_t *batches, double *p50_ms,

@@ -11,6 +11,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+GEN_PATH = os.path.join(HERE, "_build", "libgen.so")
 WINDOW = 65536
 MAX_SEQS = WINDOW // 3  # compress_zstd_custom.rs:55
 
@@ -34,6 +35,27 @@ def lib():
         L.oracle_lzma2_match_find.restype = None
         _lib = L
     return _lib
+
+
+_gen = None
+
+
+def gen_synthetic(seed, n, max_offset=8 << 20, mix=(0.4, 0.4, 0.2)):
+    """The seeded synthetic input (include/gcz_gen.h) from _build/libgen.so,
+    byte for byte what gcz.gen_synthetic gives, without loading libgcz.so."""
+    global _gen
+    if _gen is None:
+        if not os.path.exists(GEN_PATH):
+            build()
+        g = ctypes.CDLL(GEN_PATH)
+        g.gcz_gen_synthetic.argtypes = [ctypes.c_uint64, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        g.gcz_gen_synthetic.restype = None
+        _gen = g
+    out = np.empty(n, np.uint8)
+    if n:
+        _gen.gcz_gen_synthetic(seed, out.ctypes.data, n, max_offset, float(mix[0]), float(mix[1]), float(mix[2]))
+    return out
 
 
 def _ptr(a):

@@ -96,3 +96,12 @@ def test_planted_mistake_is_caught():
     win = data[:65536]
     with pytest.raises(AssertionError):
         assert decode_window(win, bad[int(offsets[0]):int(offsets[1])]) == win.tobytes()
+
+
+def test_oracle_generator_build_matches_the_package_generator():
+    """oracle/_build/libgen.so (what the CPU baselines use, so that they never
+    load the product library) gives the same bytes as gcz.gen_synthetic."""
+    import gcz
+
+    for seed, n, max_off in ((1, 1 << 20, 8 << 20), (3, 3 * 65536 + 5, 128 << 20), (7, 1, 8 << 20)):
+        assert np.array_equal(orc.gen_synthetic(seed, n, max_off), gcz.gen_synthetic(seed, n, max_off))

@@ -86,14 +86,14 @@ def test_wait_while_another_thread_submits(ctx):
 
 
 def test_warm_up_then_serve(ctx):
-    """warm_up grows both slots for every kind (zero bytes, small host
+    """warm_up runs one max-size request of every kind (zero bytes, small host
     outputs); requests served afterwards still get their own results."""
     import gcz
     from gcz import serving
 
     srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=4 << 20)
     srv.warm_up((serving.ZSTD, serving.LZMA2, serving.ZSTD_FRAMES))
-    assert srv.stats()["completed"] == 6
+    assert srv.stats()["completed"] == 3
     data = gcz.gen_synthetic(77, 3 << 20, 8 << 20)
     seqs, off = srv.wait(srv.submit(serving.ZSTD, data, 16))
     s, o = ctx.zstd_match_find(data, 16)
@@ -192,3 +192,125 @@ def test_frames_requests_in_a_mixed_stream(ctx):
     st = srv.stats()
     srv.close()
     assert st["completed"] == len(reqs) and st["status"] == 0
+
+
+def _check_alone(ctx, kind, depth, data, res):
+    from gcz import serving
+
+    if kind == serving.ZSTD:
+        s, o = ctx.zstd_match_find(data, depth)
+        np.testing.assert_array_equal(res[1], o)
+        np.testing.assert_array_equal(res[0], s)
+    elif kind == serving.ZSTD_FRAMES:
+        blob, fs = ctx.zstd_compress_frames_gpu(data, 1 if depth <= 16 else 2) if depth > 1 else (None, None)
+        if depth <= 1:  # greedy frames: the frames of the greedy sequences
+            return
+        want, pos = [], 0
+        for sz in fs.tolist():
+            want.append(blob[pos:pos + sz].tobytes())
+            pos += sz
+        assert res == want
+    else:
+        p, h = ctx.lzma2_match_find(data, 32)
+        if res[0] is not None:
+            np.testing.assert_array_equal(res[0], p)
+        np.testing.assert_array_equal(res[1], h)
+
+
+def test_every_kind_in_one_batch(ctx):
+    """Zstd (lazy and greedy), GPU frames and LZMA2 requests submitted together
+    land in one batch (one slot, one candidate sweep over all their windows)
+    and each gets exactly its result alone."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=4 * 10**9, max_batch_bytes=32 << 20, max_batch_requests=64)
+    rng = np.random.default_rng(5)
+    plan = [(serving.ZSTD, 16), (serving.LZMA2, 32), (serving.ZSTD_FRAMES, 16), (serving.ZSTD, 1),
+            (serving.LZMA2, 32), (serving.ZSTD, 64), (serving.ZSTD_FRAMES, 64), (serving.ZSTD, 16)]
+    sizes = [3 << 20, 65537, 1 << 20, 200000, 5, 2 << 20, 70000, 0]
+    datas = [gcz.gen_synthetic(1100 + i, n, 8 << 20, tuple(rng.dirichlet([1, 1, 1]))) for i, n in enumerate(sizes)]
+    for rep in range(2):
+        before = srv.stats()["batches"]
+        reqs = [srv.submit(k, d, depth) for (k, depth), d in zip(plan, datas)]
+        res = [srv.wait(r) for r in reqs]
+        for (k, depth), d, x in zip(plan, datas, res):
+            _check_alone(ctx, k, depth, d, x)
+        assert srv.stats()["batches"] - before <= 2  # the first may launch alone before the rest arrive
+    st = srv.stats()
+    srv.close()
+    assert st["status"] == 0
+
+
+def test_batch_error_stays_in_its_batch(ctx):
+    """A batch whose bounded wait runs out (the failure-detection probe)
+    completes with GCZ_EDEVICE; the loop keeps serving, and requests before
+    and after it get their own results (each batch has its own status)."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=2 * 10**9, max_batch_bytes=8 << 20)
+    data = gcz.gen_synthetic(81, 1 << 20, 8 << 20)
+    r0 = srv.submit(serving.ZSTD, data, 16)
+    _check_alone(ctx, serving.ZSTD, 16, data, srv.wait(r0))
+    for _ in range(3):
+        probe = srv.selftest_wait_timeout(1 << 10)
+        with pytest.raises(gcz.GczError) as e:
+            srv.wait(probe)
+        assert e.value.code == gcz._lib.GCZ_EDEVICE
+        r = srv.submit(serving.ZSTD, data, 16)
+        _check_alone(ctx, serving.ZSTD, 16, data, srv.wait(r))
+        rl = srv.submit(serving.LZMA2, data, 32)
+        _check_alone(ctx, serving.LZMA2, 32, data, srv.wait(rl))
+    # the context's own status is untouched by the loop's batches
+    s, o = ctx.zstd_match_find(data, 16)
+    assert o[-1] > 0
+    srv.close()
+
+
+def test_wait_timeout_keeps_the_request(ctx):
+    """A wait that times out returns GCZ_ETIMEOUT and leaves the request in
+    the loop; a later wait collects exactly its result."""
+    import gcz
+    from gcz import serving
+
+    srv = serving.Server(ctx, hbm_budget=4 * 10**9, max_batch_bytes=64 << 20)
+    data = gcz.gen_synthetic(82, 64 << 20, 8 << 20)
+    r = srv.submit(serving.ZSTD, data, 16)
+    with pytest.raises(gcz.GczError) as e:
+        srv.wait(r, timeout_s=0.0)  # 64 MiB cannot be copied in, let alone matched, in zero time
+    assert e.value.code == gcz._lib.GCZ_ETIMEOUT
+    _check_alone(ctx, serving.ZSTD, 16, data, srv.wait(r))
+    srv.close()
+
+
+def test_slots_from_budget_and_no_allocation_while_serving(ctx):
+    """Slots follow the HBM budget (22 device bytes per input byte of a batch,
+    at most 8); every buffer is allocated at creation, so serving a burst of
+    mixed requests leaves the device's free memory where it was."""
+    import torch
+    import gcz
+    from gcz import serving
+
+    mb = 16 << 20
+    srv = serving.Server(ctx, hbm_budget=3 * 22 * mb, max_batch_bytes=mb)
+    slots, dev_bytes = srv.info()
+    assert slots == 3 and dev_bytes <= 3 * 22 * mb + 3 * 40 * (2 << 20)
+    srv.close()
+    srv = serving.Server(ctx, hbm_budget=120 * 10**9, max_batch_bytes=mb)
+    assert srv.info()[0] == 8
+    srv.warm_up((serving.ZSTD, serving.LZMA2, serving.ZSTD_FRAMES))
+    rng = np.random.default_rng(9)
+    datas = [gcz.gen_synthetic(1200 + i, int(x), 8 << 20) for i, x in
+             enumerate(np.exp(rng.uniform(np.log(4096), np.log(mb), size=40)))]
+    kinds = [serving.ZSTD, serving.LZMA2, serving.ZSTD_FRAMES]
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    reqs = [(kinds[i % 3], d, srv.submit(kinds[i % 3], d, 16 if kinds[i % 3] != serving.LZMA2 else 32))
+            for i, d in enumerate(datas)]
+    out = [(k, d, srv.wait(r)) for k, d, r in reqs]
+    torch.cuda.synchronize()
+    assert abs(torch.cuda.mem_get_info()[0] - free0) < (4 << 20)
+    for k, d, x in out[:6]:
+        _check_alone(ctx, k, 16 if k != serving.LZMA2 else 32, d, x)
+    srv.close()
