@@ -105,59 +105,6 @@ struct CodeTables {
     }
 };
 
-// Encoder tables in shared memory: enc[s * size + v] = D | nbBits(D) << 6 | baseline(D) << 10
-// (16 bits: states and baselines are below 64, bit counts at most 6) for the
-// state D of symbol s whose interval holds decoder state v.
-struct FseEnc {
-    uint16_t ll[kLLSyms << kLLLog];
-    uint16_t ml[kMLSyms << kMLLog];
-    uint16_t of[kOFSyms << kOFLog];
-    uint8_t sym[64];
-    uint8_t nbits[64];
-    uint16_t base[64];
-};
-
-// Decoder table of a normalised distribution (RFC 8878 4.1.1: symbol spread,
-// then nbBits / baseline per state), turned into the encoder table above.
-__device__ void build_fse(FseEnc &t, const int8_t *norm, uint32_t nsym, uint32_t al, uint16_t *enc) {
-    const uint32_t size = 1u << al;
-    if (threadIdx.x == 0) {
-        const uint32_t mask = size - 1u, step = (size >> 1) + (size >> 3) + 3u;
-        uint32_t high = size - 1u;
-        uint16_t next[64];
-        for (uint32_t s = 0; s < nsym; ++s) {
-            if (norm[s] == -1) {
-                t.sym[high--] = static_cast<uint8_t>(s);
-                next[s] = 1;
-            } else {
-                next[s] = static_cast<uint16_t>(norm[s]);
-            }
-        }
-        uint32_t pos = 0;
-        for (uint32_t s = 0; s < nsym; ++s) {
-            for (int i = 0; i < norm[s]; ++i) {
-                t.sym[pos] = static_cast<uint8_t>(s);
-                do {
-                    pos = (pos + step) & mask;
-                } while (pos > high);
-            }
-        }
-        for (uint32_t u = 0; u < size; ++u) {
-            const uint32_t x = next[t.sym[u]]++;
-            const uint32_t nb = al - highbit(x);
-            t.nbits[u] = static_cast<uint8_t>(nb);
-            t.base[u] = static_cast<uint16_t>((x << nb) - size);
-        }
-    }
-    __syncthreads();
-    for (uint32_t u = threadIdx.x; u < size; u += blockDim.x) {
-        const uint32_t s = t.sym[u], nb = t.nbits[u], b = t.base[u];
-        const uint16_t e = static_cast<uint16_t>(u | (nb << 6) | (b << 10));
-        for (uint32_t v = b; v < b + (1u << nb); ++v) enc[s * size + v] = e;
-    }
-    __syncthreads();
-}
-
 // Forward bit writer (the decoder reads the stream backwards from its end
 // marker).  Bytes go to global memory one at a time: frame positions have no
 // alignment.
@@ -934,38 +881,214 @@ __global__ void __launch_bounds__(kLitThreads) zenc_huf_write_kernel(ZencArgs a)
 }
 
 // ---------------------------------------------------------------- sequences
-// One warp per window, kSeqWarps windows per CTA (the FSE tables are shared).
-// Sequences pass through shared memory in chunks of kChunk; the only serial
-// work -- the repeat-offset history and the three FSE state chains -- runs
-// on single lanes over shared memory, the rest is spread over the warp:
+// One warp per window, kSeqWarps windows per CTA.  Sequences pass through
+// shared memory in chunks of kChunk; the only serial work -- the
+// repeat-offset history, the three tables and the three FSE state chains --
+// runs on single lanes over shared memory, the rest is spread over the warp:
 //   R. ascending chunks: lane 0 computes each Offset_Value from the decoder's
-//      repeat history; the values go to a per-window global scratch.
+//      repeat history; the values go to a per-window global scratch; the
+//      lanes count the LL, ML and OF codes.
+//   T. lanes 0-2 pick the table of LL, OF and ML (RFC 8878 3.1.1.3.2.1):
+//      RLE_Mode when one code is used, else FSE_Compressed_Mode or
+//      Predefined_Mode, whichever costs fewer bits by an integer estimate
+//      (below); then spread the table and list each code's states.
 //   E. descending chunks (the bitstream starts with the last sequence):
 //      codes in parallel; lanes 0-2 run the LL / ML / OF chains; a warp scan
 //      gives each sequence's bit position; every lane ORs its sequences'
 //      fields into the warp's bit buffer; whole 32-bit words are stored, the
 //      partial last word carries into the next chunk.
-constexpr uint32_t kChunk = 256;
+// The cost estimate counts, per code c used k times, k * (A - log2(n_c))
+// bits, with log2 taken piecewise linear between powers of two in 1/256 bit
+// (lg256 below), plus the table description's bytes.  FSE_Compressed_Mode
+// uses accuracy A = max(5, min(Amax, bitlen(ns - 1) - 2)), raised until the
+// table has two states per used code (Amax: 9 for LL and ML, 8 for OF), and
+// counts normalised to 2^A by rounding k * 2^A / ns (at least 1); the most
+// used code takes a positive remainder, a negative one is taken one state at a
+// time from the largest count (lowest code first on ties).
+// The encoder of any table follows from its decoder (RFC 8878 4.1.1): code c
+// with normalised count n owns, in ascending decoder-state order, the states
+// numbered x = n .. 2n-1; for the next decoder state D' the encoder takes the
+// state x = (D' + 2^A) >> b, with b the bit count that puts x in [n, 2n), and
+// writes the low b bits of D' + 2^A.
+constexpr uint32_t kChunk = 128;
 constexpr uint32_t kSeqWarps = 4;
 constexpr uint32_t kPerLane = kChunk / 32;
-constexpr uint32_t kBufWords = kChunk * 65u / 32u + 4u;  // <= 65 bits per sequence, plus the carried word
+constexpr uint32_t kBufWords = kChunk * 74u / 32u + 4u;  // <= 74 bits per sequence, plus the carried word
+constexpr uint32_t kMaxAl = 9;                           // Accuracy_Log limit of LL and ML (OF: 8)
+constexpr uint32_t kTabDesc = 128;                       // bytes of one table description
+constexpr uint32_t kOFCodes = 32;                        // offset codes counted (a window's are <= 16)
+
+// One field's (LL, ML or OF) table for one window.
+struct FieldTab {
+    uint16_t stl[1u << kMaxAl];  // each code's decoder states, ascending, code after code
+    uint8_t sym[1u << kMaxAl];   // spread table (building only)
+    uint16_t cumul[64];          // first stl entry of code c
+    uint16_t norm[64];           // normalised count (>= 1 where used; "less than 1" counts as 1)
+    uint32_t hist[64];           // uses of code c in the window
+    uint8_t desc[kTabDesc];      // FSE table description, or the RLE code
+    uint32_t al;                 // accuracy log (0 for RLE_Mode)
+    uint32_t mode;               // 0 Predefined_Mode, 1 RLE_Mode, 2 FSE_Compressed_Mode
+    uint32_t desc_len;
+};
 
 struct WarpSeq {
     uint4 q[kChunk];          // the chunk's records, in bitstream order (last sequence first)
     uint32_t ov[kChunk];      // Offset_Value
     uint8_t code[3][kChunk];  // LL, ML, OF codes
-    uint16_t upd[3][kChunk];  // state-update bits: value | nbBits << 8 (LL, ML, OF)
+    uint16_t upd[3][kChunk];  // state-update bits: value | nbBits << 12 (LL, ML, OF)
     uint32_t pos[kChunk];     // bit position within the chunk
     uint32_t buf[kBufWords];
     uint32_t state[3];
+    FieldTab tab[3];          // LL, ML, OF
 };
 
 struct SeqSmem {
-    FseEnc T;
     CodeTables C;
     WarpSeq W[kSeqWarps];
 };
 static_assert(sizeof(SeqSmem) * 4 + 4 * 1024 <= 233472, "four sequence CTAs per SM");
+
+// log2(x) * 256, piecewise linear between powers of two (x >= 1).
+__device__ __forceinline__ uint32_t lg256(uint32_t x) {
+    const uint32_t h = highbit(x);
+    return 256u * h + ((x << 8) >> h) - 256u;
+}
+
+// Picks and builds field f's table from its code histogram (one lane).
+// pre: the predefined distribution (-1 = "less than 1"), pre_n codes.
+__device__ void build_field_table(FieldTab &T, uint32_t ns, uint32_t ncodes, uint32_t amax, const int8_t *pre,
+                                  uint32_t pre_n, uint32_t pre_al) {
+    uint32_t used = 0, last = 0;
+    for (uint32_t c = 0; c < ncodes; ++c)
+        if (T.hist[c]) {
+            ++used;
+            last = c;
+        }
+    if (used == 1u) {  // RLE_Mode: one code, no state
+        T.mode = 1;
+        T.al = 0;
+        T.desc[0] = static_cast<uint8_t>(last);
+        T.desc_len = 1;
+        return;
+    }
+    // Predefined cost (impossible when a used code has no predefined state).
+    uint64_t cost_pre = 0;
+    bool pre_ok = true;
+    for (uint32_t c = 0; c <= last; ++c) {
+        if (!T.hist[c]) continue;
+        if (c >= pre_n || pre[c] == 0) {
+            pre_ok = false;
+            break;
+        }
+        const uint32_t n = pre[c] < 0 ? 1u : static_cast<uint32_t>(pre[c]);
+        cost_pre += static_cast<uint64_t>(T.hist[c]) * (256u * pre_al - lg256(n));
+    }
+    // FSE_Compressed_Mode: accuracy, normalised counts, description.
+    uint32_t al = 32u - static_cast<uint32_t>(__clz(ns - 1u));  // bit length of ns - 1
+    al = al > 2u ? al - 2u : 0u;
+    al = al < amax ? al : amax;
+    al = al > 5u ? al : 5u;
+    while ((1u << al) < 2u * used && al < amax) ++al;
+    const uint32_t size = 1u << al;
+    int32_t sum = 0;
+    uint32_t top = 0;
+    for (uint32_t c = 0; c < 64u; ++c) {
+        uint32_t n = 0;
+        if (c <= last && T.hist[c]) {
+            n = (T.hist[c] * size + ns / 2u) / ns;
+            n = n > 1u ? n : 1u;
+            if (T.hist[c] > T.hist[top]) top = c;
+        }
+        T.norm[c] = static_cast<uint16_t>(n);
+        sum += static_cast<int32_t>(n);
+    }
+    int32_t d = static_cast<int32_t>(size) - sum;
+    if (d > 0) T.norm[top] = static_cast<uint16_t>(T.norm[top] + d);
+    for (; d < 0; ++d) {
+        uint32_t big = 0;
+        for (uint32_t c = 1; c <= last; ++c)
+            if (T.norm[c] > T.norm[big]) big = c;
+        T.norm[big] = static_cast<uint16_t>(T.norm[big] - 1u);
+    }
+    SmemBits wr{T.desc, kTabDesc, 0u, 0u, 0ull, false};
+    {
+        wr.add(al - 5u, 4u);
+        int remaining = static_cast<int>(size) + 1, threshold = static_cast<int>(size);
+        uint32_t nb = al + 1u;
+        for (int c = 0; c <= static_cast<int>(last); ++c) {
+            const int n = T.norm[c];
+            const int v = n + 1, mx = (2 * threshold - 1) - remaining;
+            if (v < mx) wr.add(static_cast<uint32_t>(v), nb - 1u);
+            else if (v < threshold) wr.add(static_cast<uint32_t>(v), nb);
+            else wr.add(static_cast<uint32_t>(v + mx), nb);
+            remaining -= n;
+            while (remaining < threshold) {
+                --nb;
+                threshold >>= 1;
+            }
+            if (n == 0) {
+                int z = 0;
+                while (c + 1 + z < static_cast<int>(last) && T.norm[c + 1 + z] == 0) ++z;
+                c += z;
+                for (; z >= 3; z -= 3) wr.add(3u, 2u);
+                wr.add(static_cast<uint32_t>(z), 2u);
+            }
+        }
+        wr.flush();
+    }
+    uint64_t cost_fse = 2048ull * wr.pos;
+    for (uint32_t c = 0; c <= last; ++c)
+        if (T.hist[c]) cost_fse += static_cast<uint64_t>(T.hist[c]) * (256u * al - lg256(T.norm[c]));
+    const bool fse = !wr.ovf && (!pre_ok || cost_fse < cost_pre);
+    uint32_t high = 0;
+    if (fse) {
+        T.mode = 2;
+        T.al = al;
+        T.desc_len = wr.pos;
+        high = size - 1u;
+    } else {  // Predefined_Mode
+        T.mode = 0;
+        T.al = pre_al;
+        T.desc_len = 0;
+        high = (1u << pre_al) - 1u;
+        for (uint32_t c = 0; c < 64u; ++c) T.norm[c] = c < pre_n ? static_cast<uint16_t>(pre[c] < 0 ? 1 : pre[c]) : 0;
+    }
+    // Spread (RFC 8878 4.1.1): "less than 1" codes at the top, the others
+    // stepped through the remaining states.
+    const uint32_t tsize = 1u << T.al, mask = tsize - 1u, step = (tsize >> 1) + (tsize >> 3) + 3u;
+    const uint32_t ntab = fse ? last + 1u : pre_n;
+    for (uint32_t c = 0; c < ntab; ++c)
+        if (!fse && pre[c] < 0) T.sym[high--] = static_cast<uint8_t>(c);
+    uint32_t pos = 0;
+    for (uint32_t c = 0; c < ntab; ++c) {
+        const int n = fse ? static_cast<int>(T.norm[c]) : static_cast<int>(pre[c]);
+        for (int i = 0; i < n; ++i) {
+            T.sym[pos] = static_cast<uint8_t>(c);
+            do {
+                pos = (pos + step) & mask;
+            } while (pos > high);
+        }
+    }
+    uint32_t acc = 0;
+    for (uint32_t c = 0; c < 64u; ++c) {
+        T.cumul[c] = static_cast<uint16_t>(acc);
+        acc += T.norm[c];
+    }
+    uint16_t fill[64];
+    for (uint32_t c = 0; c < 64u; ++c) fill[c] = T.cumul[c];
+    for (uint32_t u = 0; u < tsize; ++u) T.stl[fill[T.sym[u]]++] = static_cast<uint16_t>(u);
+}
+
+// Decoder state before code c when the next decoder state is dn: the state
+// and, in `up`, the bits the decoder reads (value | count << 12).
+__device__ __forceinline__ uint32_t fse_encode(const FieldTab &T, uint32_t c, uint32_t dn, uint16_t &up) {
+    const uint32_t n = T.norm[c], v = dn + (1u << T.al);
+    const uint32_t hi = T.al - highbit(n);
+    const uint32_t nb = v >= (n << hi) ? hi : hi - 1u;
+    const uint32_t x = v >> nb;
+    up = static_cast<uint16_t>((v - (x << nb)) | (nb << 12));
+    return T.stl[T.cumul[c] + x - n];
+}
 
 __device__ __forceinline__ void or_bits(uint32_t *buf, uint32_t bitpos, uint64_t v, uint32_t nb) {
     if (nb == 0u) return;
@@ -985,7 +1108,9 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
     const uint4 *sq = a.seqs + s0;
     uint32_t *ovg = a.ovs + static_cast<uint64_t>(b) * kZencMaxSeqs;
 
-    // ---- R: Offset_Values, ascending, with the decoder's repeat history (lane 0)
+    for (uint32_t k = lane; k < 64u; k += 32u) S.tab[0].hist[k] = S.tab[1].hist[k] = S.tab[2].hist[k] = 0u;
+    __syncwarp();
+    // ---- R: Offset_Values, ascending, with the decoder's repeat history (lane 0); code counts
     uint32_t r1 = 1, r2 = 4, r3 = 8;
     for (uint32_t lo = 0; lo < ns; lo += kChunk) {
         const uint32_t len = min(kChunk, ns - lo);
@@ -993,6 +1118,8 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
             const uint4 q = sq[lo + k];
             S.pos[k] = q.x;               // offset
             S.ov[k] = q.y == 0u ? 1u : 0u;  // literal length is zero
+            atomicAdd(&S.tab[0].hist[G.C.ll_code(q.y)], 1u);
+            atomicAdd(&S.tab[1].hist[G.C.ml_code(q.z)], 1u);
         }
         __syncwarp();
         if (lane == 0) {
@@ -1015,13 +1142,24 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
             }
         }
         __syncwarp();
-        for (uint32_t k = lane; k < len; k += 32u) ovg[lo + k] = S.ov[k];
+        for (uint32_t k = lane; k < len; k += 32u) {
+            ovg[lo + k] = S.ov[k];
+            atomicAdd(&S.tab[2].hist[highbit(S.ov[k])], 1u);
+        }
         __syncwarp();
     }
 
-    // ---- E: the bitstream, last sequence first
+    // ---- T: the three tables (lane 0: LL, lane 1: ML, lane 2: OF)
+    if (lane == 0) build_field_table(S.tab[0], ns, kLLSyms, kMaxAl, kLLNorm, kLLSyms, kLLLog);
+    else if (lane == 1) build_field_table(S.tab[1], ns, kMLSyms, kMaxAl, kMLNorm, kMLSyms, kMLLog);
+    else if (lane == 2) build_field_table(S.tab[2], ns, kOFCodes, 8u, kOFNorm, kOFSyms, kOFLog);
+    __syncwarp();
+
+    // ---- header: Number_of_Sequences, modes, table descriptions (LL, OF, ML)
     uint8_t *hp = slot + sec;
-    const uint32_t hl = ns < 128u ? 2u : 3u;  // Number_of_Sequences (1-2 bytes) + modes byte
+    const uint32_t nsb = ns < 128u ? 1u : 2u;
+    const uint32_t d_ll = S.tab[0].desc_len, d_of = S.tab[2].desc_len, d_ml = S.tab[1].desc_len;
+    const uint32_t hl = nsb + 1u + d_ll + d_of + d_ml;
     if (lane == 0) {
         if (ns < 128u) {
             hp[0] = static_cast<uint8_t>(ns);
@@ -1029,11 +1167,17 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
             hp[0] = static_cast<uint8_t>((ns >> 8) + 0x80u);
             hp[1] = static_cast<uint8_t>(ns);
         }
-        hp[hl - 1] = 0;  // Predefined_Mode for all three
+        hp[nsb] = static_cast<uint8_t>((S.tab[0].mode << 6) | (S.tab[2].mode << 4) | (S.tab[1].mode << 2));
+    }
+    for (uint32_t k = lane; k < d_ll + d_of + d_ml; k += 32u) {
+        const uint8_t v = k < d_ll ? S.tab[0].desc[k]
+                                   : (k < d_ll + d_of ? S.tab[2].desc[k - d_ll] : S.tab[1].desc[k - d_ll - d_of]);
+        hp[nsb + 1u + k] = v;
     }
     uint8_t *bs = hp + hl;
     // bitstream bytes at which the block stops paying (none when the literals alone fill the window)
     const int32_t room = static_cast<int32_t>(fh + 3u + w) - static_cast<int32_t>(sec + hl);
+    if (room <= 0) return 0u;
     uint32_t carry_word = 0, carry_bits = 0, out_pos = 0;
     uint32_t D = 0;  // chain state of lanes 0-2
     for (uint32_t hi = ns; hi > 0u;) {
@@ -1052,20 +1196,20 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
         for (uint32_t k = lane; k < kBufWords; k += 32u) S.buf[k] = 0u;
         __syncwarp();
         if (lane < 3u) {  // the three FSE chains
-            const uint32_t lg = lane == 2u ? kOFLog : kLLLog;
-            const uint16_t *enc = lane == 0u ? G.T.ll : (lane == 1u ? G.T.ml : G.T.of);
+            const FieldTab &T = S.tab[lane];
             const uint8_t *cd = S.code[lane];
             uint16_t *up = S.upd[lane];
             uint32_t j = 0;
-            if (hi == ns) {  // last sequence: any state of its symbol, no bits
-                D = enc[static_cast<uint32_t>(cd[0]) << lg] & 63u;
-                up[0] = 0;
-                j = 1;
-            }
-            for (; j < len; ++j) {
-                const uint32_t e = enc[(static_cast<uint32_t>(cd[j]) << lg) + D];
-                up[j] = static_cast<uint16_t>((D - (e >> 10)) | (((e >> 6) & 15u) << 8));
-                D = e & 63u;
+            if (T.mode == 1u) {  // RLE_Mode: no state, no bits
+                for (; j < len; ++j) up[j] = 0;
+            } else {
+                if (hi == ns) {  // last sequence: any state of its code, no bits
+                    uint16_t dummy;
+                    D = fse_encode(T, cd[0], 0u, dummy);
+                    up[0] = 0;
+                    j = 1;
+                }
+                for (; j < len; ++j) D = fse_encode(T, cd[j], D, up[j]);
             }
         }
         __syncwarp();
@@ -1076,7 +1220,7 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
             const uint32_t j = j0 + u;
             uint32_t nb = 0;
             if (j < len) {
-                nb = (S.upd[0][j] >> 8) + (S.upd[1][j] >> 8) + (S.upd[2][j] >> 8) + G.C.ll_bits[S.code[0][j]] +
+                nb = (S.upd[0][j] >> 12) + (S.upd[1][j] >> 12) + (S.upd[2][j] >> 12) + G.C.ll_bits[S.code[0][j]] +
                      G.C.ml_bits[S.code[1][j]] + S.code[2][j];
             }
             S.pos[j] = wsum;
@@ -1097,9 +1241,9 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
             const uint32_t p0 = base + S.pos[j];
             // updates: OF, ML, LL (the decoder, reading backwards, takes LL, ML, OF)
             const uint32_t uo = S.upd[2][j], um = S.upd[1][j], ul = S.upd[0][j];
-            const uint32_t no = uo >> 8, nm = um >> 8, nl = ul >> 8;
-            const uint64_t ga = static_cast<uint64_t>(uo & 0xFFu) | (static_cast<uint64_t>(um & 0xFFu) << no) |
-                                (static_cast<uint64_t>(ul & 0xFFu) << (no + nm));
+            const uint32_t no = uo >> 12, nm = um >> 12, nl = ul >> 12;
+            const uint64_t ga = static_cast<uint64_t>(uo & 0xFFFu) | (static_cast<uint64_t>(um & 0xFFFu) << no) |
+                                (static_cast<uint64_t>(ul & 0xFFFu) << (no + nm));
             or_bits(S.buf, p0, ga, no + nm + nl);
             // extra bits: LL, ML, OF
             const uint4 q = S.q[j];
@@ -1127,9 +1271,9 @@ __device__ uint32_t encode_sequences_warp(const ZencArgs &a, const SeqSmem &G, W
     uint32_t content = 0;
     if (lane == 0) {
         BitWriter bw{bs, out_pos, carry_word, carry_bits};
-        bw.add(S.state[1], kMLLog);
-        bw.add(S.state[2], kOFLog);
-        bw.add(S.state[0], kLLLog);
+        bw.add(S.state[1], S.tab[1].al);
+        bw.add(S.state[2], S.tab[2].al);
+        bw.add(S.state[0], S.tab[0].al);
         bw.close();
         content = sec + hl + bw.pos - (fh + 3u);
     }
@@ -1142,9 +1286,7 @@ __global__ void __launch_bounds__(32 * kSeqWarps) zenc_sequences_kernel(ZencArgs
     SeqSmem &G = *reinterpret_cast<SeqSmem *>(smem_raw);
     const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
     G.C.build();
-    build_fse(G.T, kLLNorm, kLLSyms, kLLLog, G.T.ll);
-    build_fse(G.T, kMLNorm, kMLSyms, kMLLog, G.T.ml);
-    build_fse(G.T, kOFNorm, kOFSyms, kOFLog, G.T.of);
+    __syncthreads();
     for (uint32_t b = blockIdx.x * kSeqWarps + wid; b < a.num_windows; b += gridDim.x * kSeqWarps) {
         const uint32_t w = win_size(a, b);
         const uint32_t fh = frame_header_bytes(w);

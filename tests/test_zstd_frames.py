@@ -63,6 +63,45 @@ def test_reference_frames_decode_with_libzstd(spec):
         assert codecs.zstd_decompress(f, win.size) == win.tobytes()
 
 
+def test_reference_frames_use_every_table_mode():
+    """Across these inputs the sequence fields get all three table modes:
+    RLE (one sequence), FSE-compressed (most windows) and predefined (few
+    sequences with many distinct codes, where a description costs more than
+    it saves)."""
+    from gcz import codecs
+
+    for k in zr.MODE_USES:
+        zr.MODE_USES[k] = 0
+    for spec in INPUTS + [{"kind": "synthetic", "n": 2000, "seed": 9}, {"kind": "text", "n": 3000, "seed": 10}]:
+        data = _build(spec)
+        for b, f in enumerate(_ref_frames(data)):
+            win = data[b * W:(b + 1) * W]
+            assert codecs.zstd_decompress(f, win.size) == win.tobytes()
+    assert all(v > 0 for v in zr.MODE_USES.values()), zr.MODE_USES
+
+
+def test_reference_frames_ratio_within_a_tenth_of_a_point_of_libzstd():
+    """On the bench generator's data the frames' size is within 0.1 percentage
+    point of libzstd's own frames for the same sequences (ZSTD_compressSequences
+    per window, the reference's coder loop)."""
+    import gcz
+    from gcz import codecs
+
+    data = gcz.gen_synthetic(2, 2 << 20, 8 << 20)
+    seqs, off = orc.zstd_sequences(data, 64)
+    comp = codecs.SequenceCompressor()
+    ours = ref = 0
+    for b in range(off.size - 1):
+        win = data[b * W:(b + 1) * W]
+        s = seqs[int(off[b]):int(off[b + 1])]
+        ref += len(comp.compress(win, s))
+        f = zr.encode_frame(win.tobytes(), [(x[0], x[1], x[2]) for x in s])
+        assert codecs.zstd_decompress(f, win.size) == win.tobytes()
+        ours += len(f)
+    comp.close()
+    assert 100.0 * (ours - ref) / data.size <= 0.1, (ours / data.size, ref / data.size)
+
+
 def _split(blob, sizes):
     out, pos = [], 0
     for s in sizes.tolist():

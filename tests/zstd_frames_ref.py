@@ -1,9 +1,10 @@
 """Pure-Python restatement of the GPU Zstd entropy stage (test checker only):
 one frame per window from its ZSTD_Sequence records, following RFC 8878 --
 single-segment frame header, one block, literals raw, RLE or Huffman-coded
-(whichever is smallest), sequences in Predefined_Mode with repeat-offset codes
--- or a raw block when the compressed block would not be smaller than the
-window.  The tests compare the GPU frames
+(whichever is smallest), sequences with repeat-offset codes and, per field
+(LL, OF, ML), an RLE, FSE-compressed or predefined table chosen by the GPU's
+integer cost estimate -- or a raw block when the compressed block would not be
+smaller than the window.  The tests compare the GPU frames
 with these byte for byte and decode both with stock libzstd."""
 
 LL_NORM = [4, 3, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 2, 1, 1, 1, 2, 2, 2, 2, 2, 2, 2, 2, 2, 3, 2, 1, 1, 1, 1, 1,
@@ -308,6 +309,52 @@ def literals_section(lits):
     return out if len(out) < len(raw) else raw
 
 
+def _lg256(x):
+    """log2(x) * 256, piecewise linear between powers of two (integer)."""
+    h = x.bit_length() - 1
+    return 256 * h + ((x << 8) >> h) - 256
+
+
+def _seq_table(hist, pre_norm, pre_log, amax):
+    """The table of one sequence field (RFC 8878 3.1.1.3.2.1): ("rle", code),
+    ("fse", norm, accuracy, description) or ("pre",), by the same integer cost
+    estimate as the GPU: k * (A * 256 - lg256(n)) per code used k times with
+    normalised count n, plus 2048 per description byte."""
+    ns = sum(hist)
+    used = [c for c, k in enumerate(hist) if k]
+    if len(used) == 1:
+        return ("rle", used[0])
+    last = used[-1]
+    pre_ok = all(c < len(pre_norm) and pre_norm[c] != 0 for c in used)
+    cost_pre = sum(hist[c] * (256 * pre_log - _lg256(1 if pre_norm[c] < 0 else pre_norm[c])) for c in used) \
+        if pre_ok else None
+    al = max(5, min(amax, max((ns - 1).bit_length() - 2, 0)))
+    while (1 << al) < 2 * len(used) and al < amax:
+        al += 1
+    size = 1 << al
+    norm = [0] * (last + 1)
+    for c in used:
+        norm[c] = max(1, (hist[c] * size + ns // 2) // ns)
+    top = max(used, key=lambda c: (hist[c], -c))
+    d = size - sum(norm)
+    if d > 0:
+        norm[top] += d
+    while d < 0:
+        big = max(range(last + 1), key=lambda c: (norm[c], -c))
+        norm[big] -= 1
+        d += 1
+    bits = _Bits()
+    _ncount_bits(norm, al, bits)
+    desc = bits.v.to_bytes((bits.n + 7) // 8, "little")
+    cost_fse = 2048 * len(desc) + sum(hist[c] * (256 * al - _lg256(norm[c])) for c in used)
+    if len(desc) <= 128 and (cost_pre is None or cost_fse < cost_pre):
+        return ("fse", norm, al, desc)
+    return ("pre",)
+
+
+MODE_USES = {"rle": 0, "fse": 0, "pre": 0}  # tables chosen so far (for the tests' coverage checks)
+
+
 def encode_frame(win, seqs):
     """win: bytes of one window; seqs: iterable of (offset, litLength, matchLength)."""
     win = bytes(win)
@@ -325,7 +372,6 @@ def encode_frame(win, seqs):
     lsec = literals_section(lits)
     ns = len(seqs)
     sh = bytes([ns]) if ns < 128 else bytes([(ns >> 8) + 0x80, ns & 0xFF])
-    sh += b"\x00"
     # repeat codes with the decoder's history
     r1, r2, r3 = 1, 4, 8
     ovs = []
@@ -343,31 +389,53 @@ def encode_frame(win, seqs):
             elif idx >= 2:
                 r1, r2, r3 = o, r1, r2
         ovs.append(v)
+    lcs = [_code(LL_BASE, ll) for _, ll, _ in seqs]
+    mcs = [_code(ML_BASE, ml) for _, _, ml in seqs]
+    ocs = [v.bit_length() - 1 for v in ovs]
+    # tables: LL, OF, ML (the order of the modes byte and of the descriptions)
+    modes, descs, enc, logs = 0, b"", {}, {}
+    for key, codes, ncodes, pre, pre_log, amax, shift, pre_enc in (
+            ("ll", lcs, 36, LL_NORM, LL_LOG, 9, 6, ENC_LL), ("of", ocs, 32, OF_NORM, OF_LOG, 8, 4, ENC_OF),
+            ("ml", mcs, 53, ML_NORM, ML_LOG, 9, 2, ENC_ML)):
+        hist = [0] * ncodes
+        for c in codes:
+            hist[c] += 1
+        t = _seq_table(hist, pre, pre_log, amax)
+        MODE_USES[t[0]] += 1
+        if t[0] == "rle":
+            modes |= 1 << shift
+            descs += bytes([t[1]])
+            enc[key], logs[key] = None, 0
+        elif t[0] == "fse":
+            modes |= 2 << shift
+            descs += t[3]
+            enc[key], logs[key] = _fse(t[1], t[2]), t[2]
+        else:
+            enc[key], logs[key] = pre_enc, pre_log
+    sh += bytes([modes]) + descs
     bits = _Bits()
-    dll = dml = dof = 0
+    st = {"ll": 0, "ml": 0, "of": 0}
     for i in range(ns - 1, -1, -1):
         _, ll, ml = seqs[i]
         v = ovs[i]
-        lc, mc, oc = _code(LL_BASE, ll), _code(ML_BASE, ml), v.bit_length() - 1
-        if i == ns - 1:
-            dll, dml, dof = ENC_LL[(lc, 0)][0], ENC_ML[(mc, 0)][0], ENC_OF[(oc, 0)][0]
+        lc, mc, oc = lcs[i], mcs[i], ocs[i]
+        code = {"ll": lc, "ml": mc, "of": oc}
+        if i == ns - 1:  # any state of the code, no bits
+            for k in ("ll", "ml", "of"):
+                st[k] = enc[k][(code[k], 0)][0] if enc[k] is not None else 0
         else:
-            for enc, cur, code in ((ENC_OF, "of", oc), (ENC_ML, "ml", mc), (ENC_LL, "ll", lc)):
-                d = {"of": dof, "ml": dml, "ll": dll}[cur]
-                u, nb, base = enc[(code, d)]
-                bits.add(d - base, nb)
-                if cur == "of":
-                    dof = u
-                elif cur == "ml":
-                    dml = u
-                else:
-                    dll = u
+            for k in ("of", "ml", "ll"):
+                if enc[k] is None:  # RLE_Mode: no state, no bits
+                    continue
+                u, nb, base = enc[k][(code[k], st[k])]
+                bits.add(st[k] - base, nb)
+                st[k] = u
         bits.add(ll - LL_BASE[lc], LL_BITS[lc])
         bits.add(ml - ML_BASE[mc], ML_BITS[mc])
         bits.add(v - (1 << oc), oc)
-    bits.add(dml, ML_LOG)
-    bits.add(dof, OF_LOG)
-    bits.add(dll, LL_LOG)
+    bits.add(st["ml"], logs["ml"])
+    bits.add(st["of"], logs["of"])
+    bits.add(st["ll"], logs["ll"])
     content = lsec + sh + bits.close()
     if len(content) >= w:
         return raw
