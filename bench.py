@@ -52,8 +52,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-configs", action="store_true", help="skip the other configs' keys (zstd_l1_16mib, ...)")
     ap.add_argument("--no-heavy-configs", action="store_true", help="skip the uneven-batch and serving keys")
+    ap.add_argument("--untuned", action="store_true", help="library default schedule, not gcz/tuned/<GPU>.json")
     ap.add_argument("--algo", type=int, default=2, help="1: fused single-warp kernels, 2: sweep + second stage")
-    ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2", "serving", "uneven", "frames"],
+    ap.add_argument("--workload", default="zstd", choices=["zstd", "lzma2", "serving", "uneven", "frames", "tune"],
                     help="zstd: Zstd L2 batched 1 GiB (the reported line); lzma2: LZMA2 L1 1 GiB, seed 3; "
                          "serving: open-loop request stream; uneven: many files in one launch")
     ap.add_argument("--rate", type=float, default=2000.0, help="serving: requests per second (Poisson)")
@@ -268,6 +269,23 @@ def link_time(torch, dev, h_in, d_in, h_out, d_out, out_bytes, piece=64 << 20, r
     return sum(times) / len(times)
 
 
+def load_tuned(ctx, args):
+    """The schedule the autotuner saved for this GPU model (gcz/tuned/), or the
+    library defaults; --algo 1 forces the fused kernels.  Returns the knobs
+    in effect."""
+    from gcz import autotune
+
+    src = "defaults"
+    if args.algo == 2 and not args.untuned:
+        if autotune.apply_tuned(ctx) is not None:
+            src = "gcz/tuned/" + os.path.basename(autotune.tuned_path(ctx.device))
+    ctx.set_option("algo", args.algo)
+    knobs = {k: ctx.query(k) for k in ("algo", "sweep_warps", "parse_seg", "parse_ctas", "lzma_ctas",
+                                       "slice_windows")}
+    knobs["source"] = src
+    return knobs
+
+
 def time_steps(torch, stream, steps, fn, flush=None):
     """Mean milliseconds per call of fn() with CUDA events on `stream`.  With no
     `flush`, one event pair brackets all steps (inputs larger than L2).  With a
@@ -408,7 +426,7 @@ def run_gcz(args):
     world, rank, local, dist = dist_setup(args)
     dev = torch.device("cuda", local)
     ctx = gcz.Context(local)
-    ctx.set_option("algo", args.algo)
+    tuned = load_tuned(ctx, args)
     n = args.bytes
     data = gcz.gen_synthetic(SEED + 1000 * rank, n, 8 << 20)
     B = gcz.num_windows(n)
@@ -530,7 +548,7 @@ def run_gcz(args):
                         "on the launch stream; e2e is the same step through the host-buffer call",
             "config": {"workload": WORKLOAD, "input_bytes_per_gpu": n, "windows_per_gpu": B, "window": 65536,
                        "search_depth": DEPTH, "sequences_per_gpu": nseq, "parallelism": f"replicas{world}",
-                       "algo": args.algo, "fallback_windows": ctx.query("fallback_windows"),
+                       "algo": args.algo, "schedule": tuned, "fallback_windows": ctx.query("fallback_windows"),
                        "l2": "input 1 GiB > 126 MB L2, no flush needed"},
             "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": n,
                     "d2h_bytes_per_step": 16 * nseq + 8 * (B + 1),
@@ -688,8 +706,9 @@ def run_lzma2(args):
     world, rank, local, dist = dist_setup(args)
     dev = torch.device("cuda", local)
     ctx = gcz.Context(local)
-    ctx.set_option("algo", args.algo)
+    tuned = load_tuned(ctx, args)
     line = measure_lzma2(args, ctx, torch, dev, dist, world, rank, local, cpu_legs=not args.no_cpu_baseline)
+    line["config"]["schedule"] = tuned
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -1171,9 +1190,27 @@ def run_frames(args):
         "gpu_launches": int(launches)}), flush=True)
 
 
+def run_tune(args):
+    """Runs the autotuner (gcz/autotune.py) on samples of the Zstd (seed 2)
+    and LZMA2 (seed 3) workloads and saves the winners for this GPU model."""
+    import torch
+    import gcz
+    from gcz import autotune
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = gcz.Context(local)
+    n = min(args.bytes, 256 << 20)
+    out = autotune.tune(ctx, gcz.gen_synthetic(SEED, n, 8 << 20), gcz.gen_synthetic(3, n, 128 << 20),
+                        search_depth=DEPTH, reps=5)
+    print(json.dumps({"workload": "tune", "sample_bytes": n, "best": out["best"], "saved": autotune.tuned_path(local),
+                      "zstd": out["zstd"]["results"], "lzma2": out["lzma2"]["results"],
+                      "host": out.get("host", {}).get("results")}), flush=True)
+
+
 def main():
     args = parse()
-    single = args.workload in ("serving", "uneven", "frames")
+    single = args.workload in ("serving", "uneven", "frames", "tune")
     if args.impl != "reference" and single and int(os.environ.get("RANK", "0")) != 0:
         return  # one-GPU workloads: rank 0 runs and prints, the other ranks have no work
     if args.impl == "reference":
@@ -1186,6 +1223,8 @@ def main():
         run_uneven(args)
     elif args.workload == "frames":
         run_frames(args)
+    elif args.workload == "tune":
+        run_tune(args)
     else:
         run_gcz(args)
 

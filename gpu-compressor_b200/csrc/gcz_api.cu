@@ -72,6 +72,9 @@ struct gcz_ctx {
     int staged = 1;
     int algo = 2;          // 1: fused single-warp kernels, 2: candidate sweep + second stage
     int parse_ctas = 3;    // second-stage CTAs per SM
+    int seg_width = 4096;  // Zstd speculative segment bytes per warp (2048, 4096, 8192)
+    int sweep_warps = 7;   // candidate-sweep windows per CTA (4-7)
+    int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM
     // profiling
     bool prof = false;
     std::vector<EventPair> events;
@@ -217,7 +220,7 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
     ProfScope ps(c, st);
     if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
-        GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st, wins));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st, wins, c->sweep_warps));
         gcz::Zstd2Launch l{};
         l.src = d_src;
         l.cand = cand;
@@ -232,6 +235,7 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
         l.status = c->d_status;
         l.num_sms = c->num_sms;
         l.ctas_per_sm = c->parse_ctas;
+        l.seg_width = (uint32_t)c->seg_width;
         l.wins = wins;
         GCZ_CUDA(c, gcz::launch_zstd_parse(l, st));
         c->all_launches += 2;
@@ -265,8 +269,11 @@ int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st)
     ProfScope ps(c, st);
     if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
-        GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st, l.wins));
-        GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, st));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st, l.wins,
+                                           c->sweep_warps));
+        gcz::LzmaLaunch lv = l;
+        lv.ctas_per_sm = c->lzma_ctas;
+        GCZ_CUDA(c, gcz::launch_lzma_verify(lv, cand, st));
         c->all_launches += 2;
     } else {
         GCZ_CUDA(c, gcz::launch_lzma_match(l, st));
@@ -431,6 +438,18 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->parse_ctas = (int)value;
         return GCZ_OK;
     }
+    if (!strcmp(key, "parse_seg") && (value == 2048 || value == 4096 || value == 8192)) {
+        c->seg_width = (int)value;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "sweep_warps") && value >= 4 && value <= 7) {
+        c->sweep_warps = (int)value;
+        return GCZ_OK;
+    }
+    if (!strcmp(key, "lzma_ctas") && value >= 1 && value <= 8) {
+        c->lzma_ctas = (int)value;
+        return GCZ_OK;
+    }
     return fail(c, GCZ_EINVAL, "unknown option '%s'", key);
 }
 
@@ -456,6 +475,18 @@ extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
         *value = c->algo;
         return GCZ_OK;
     }
+    const struct {
+        const char *k;
+        long v;
+    } knobs[] = {{"staged", c->staged},          {"parse_ctas", c->parse_ctas},
+                 {"parse_seg", c->seg_width},    {"sweep_warps", c->sweep_warps},
+                 {"lzma_ctas", c->lzma_ctas},    {"slice_windows", (long)c->slice_windows},
+                 {"frames_slice_windows", (long)c->frames_slice_windows}};
+    for (const auto &kv : knobs)
+        if (!strcmp(key, kv.k)) {
+            *value = kv.v;
+            return GCZ_OK;
+        }
     if (!strcmp(key, "fallback_windows")) {  // windows whose speculative parse fell back (since creation)
         DeviceGuard g(c->device);
         uint32_t h[2] = {0, 0};
@@ -732,7 +763,8 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
         if ((r = ensure_dev(c, c->sc.seg, gcz::zstd2_seg_scratch_entries((uint32_t)nb) * 8)) != GCZ_OK) return r;
         ProfScope ps(c, st);
         uint16_t *cand = static_cast<uint16_t *>(c->sc.cand.p);
-        GCZ_CUDA(c, gcz::launch_cand_sweep(d_input, n_eff, chunk_size, (uint32_t)nb, cand, c->num_sms, st));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(d_input, n_eff, chunk_size, (uint32_t)nb, cand, c->num_sms, st, nullptr,
+                                           c->sweep_warps));
         gcz::Zstd2Launch l{};
         l.src = d_input;
         l.cand = cand;
@@ -748,6 +780,7 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
         l.status = c->d_status;
         l.num_sms = c->num_sms;
         l.ctas_per_sm = c->parse_ctas;
+        l.seg_width = (uint32_t)c->seg_width;
         GCZ_CUDA(c, gcz::launch_zstd_parse(l, st));
         c->all_launches += 2;
     } else {
@@ -1129,10 +1162,10 @@ double now_ms() {
 
 // Device bytes per input byte of one slot, pre-sized at creation for a batch of
 // max_batch_bytes of any mix of kinds: slab 1, candidates 2, Zstd speculative
-// lists 3.25, packed sequences 2.67, ZSTD_Sequence output 5.33, LZMA2 packed
+// lists 3.9 (sized for the widest segment layout), packed sequences 2.67, ZSTD_Sequence output 5.33, LZMA2 packed
 // matches 4, and for frames the frames 1.02, frame slots 1.02, offset codes
 // 1.33 and plans 0.03.
-constexpr double kDeviceBytesPerInputByte = 22.0;
+constexpr double kDeviceBytesPerInputByte = 23.0;
 constexpr int kMaxServerSlots = 8;
 
 // Request groups, in window order inside a batch: every group's windows are one
@@ -1315,7 +1348,7 @@ int server_launch(gcz_server *sv, ServerSlot &s) {
         if (q->n) GCZ_CUDA(c, cudaMemcpyAsync(slab_p + q->slab_off, q->src, q->n, cudaMemcpyHostToDevice, s.st));
     if (nb) {
         GCZ_CUDA(c, cudaMemcpyAsync(s.wins.p, s.hwins.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, s.st));
-        GCZ_CUDA(c, gcz::launch_cand_sweep(slab_p, slab, kW, (uint32_t)nb, cand, c->num_sms, s.st, dw));
+        GCZ_CUDA(c, gcz::launch_cand_sweep(slab_p, slab, kW, (uint32_t)nb, cand, c->num_sms, s.st, dw, c->sweep_warps));
     }
     const uint32_t nz = s.wb[kGrpLzma];  // Zstd windows: sequences and frames groups
     uint64_t *d_off = static_cast<uint64_t *>(s.offsets.p);
@@ -1338,6 +1371,8 @@ int server_launch(gcz_server *sv, ServerSlot &s) {
             l.status = status;
             l.num_sms = c->num_sms;
             l.ctas_per_sm = c->parse_ctas;
+            l.seg_width = (uint32_t)c->seg_width;
+        l.seg_width = (uint32_t)c->seg_width;
             l.wins = dw + a;
             GCZ_CUDA(c, gcz::launch_zstd_parse(l, s.st));
         }
@@ -1388,6 +1423,7 @@ int server_launch(gcz_server *sv, ServerSlot &s) {
         l.num_sms = c->num_sms;
         l.staged = 1;
         l.wins = dw + l0;
+        l.ctas_per_sm = c->lzma_ctas;
         GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, s.st));
         for (ServerReq *q : s.reqs) {
             if (q->group != kGrpLzma || !q->n) continue;
@@ -1588,7 +1624,7 @@ extern "C" int gcz_server_create(gcz_ctx *c, uint64_t hbm_budget, uint64_t max_b
                                  uint32_t max_batch_requests, gcz_server **out) {
     if (!c || !out) return GCZ_EINVAL;
     *out = nullptr;
-    // Slot count and batch size from the budget: each slot holds ~22 device
+    // Slot count and batch size from the budget: each slot holds ~23 device
     // bytes per input byte of a max-size batch.  With no batch size given, the
     // budget is split over four slots.
     const uint64_t per_byte_budget = (uint64_t)(hbm_budget / kDeviceBytesPerInputByte);

@@ -46,6 +46,7 @@ struct LzmaLaunch {
     int num_sms;
     int staged;
     const WinDesc *wins = nullptr;  // optional window table (second stage only)
+    int ctas_per_sm = 3;            // second-stage CTAs per SM (schedule only)
 };
 
 // Second-stage Zstd parse after the candidate sweep.
@@ -66,11 +67,13 @@ struct Zstd2Launch {
     int num_sms;
     int ctas_per_sm;
     const WinDesc *wins;    // optional window table (null: windows at window * w)
+    uint32_t seg_width = 4096;  // speculative segment bytes per warp: 2048, 4096 or 8192 (schedule only)
 };
 
 cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
+// sweep_warps: windows swept per CTA (4-7, one 32 KiB table each; schedule only).
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st, const WinDesc *wins = nullptr);
+                              int num_sms, cudaStream_t st, const WinDesc *wins = nullptr, int sweep_warps = 7);
 size_t zstd2_seg_scratch_entries(uint32_t num_windows);
 cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st);
 cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);

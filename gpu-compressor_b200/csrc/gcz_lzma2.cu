@@ -414,7 +414,7 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     static SmemOnce smem_set_3{0};
     cudaError_t e = set_smem_once(lzma_verify_kernel, smem, smem_set_3);
     if (e != cudaSuccess) return e;
-    int grid = l.num_sms * 3;
+    int grid = l.num_sms * (l.ctas_per_sm > 0 ? l.ctas_per_sm : 3);
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
     lzma_verify_kernel<<<grid, kL2Threads, smem, st>>>(a);
     return cudaGetLastError();

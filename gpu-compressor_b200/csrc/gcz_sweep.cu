@@ -25,7 +25,6 @@
 namespace gcz {
 namespace {
 
-constexpr int kSweepWarpsPerCta = 7;  // 7 x 32 KiB tables per SM
 
 struct SweepArgs {
     const uint8_t *src;
@@ -36,6 +35,9 @@ struct SweepArgs {
     const WinDesc *wins;
 };
 
+// kSweepWarpsPerCta windows per CTA, one 32 KiB table each (7 fill an SM's
+// shared memory); a schedule knob, the candidates do not depend on it.
+template <int kSweepWarpsPerCta>
 __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -134,18 +136,33 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
 
 }  // namespace
 
+namespace {
+template <int kWarps>
+cudaError_t launch_sweep_variant(const SweepArgs &a, int num_sms, cudaStream_t st) {
+    const uint32_t smem = kWarps * kHashSize * sizeof(uint16_t);
+    static SmemOnce smem_set{0};
+    cudaError_t e = set_smem_once(cand_sweep_kernel<kWarps>, smem, smem_set);
+    if (e != cudaSuccess) return e;
+    // as many CTAs per SM as the tables allow (one for 5-7 warps, two for 4 or less)
+    const uint32_t per_sm = (227u * 1024u) / (smem + 1024u);
+    uint32_t ctas = (a.num_windows + kWarps - 1) / kWarps;
+    const uint32_t cap = static_cast<uint32_t>(num_sms) * (per_sm ? per_sm : 1u);
+    if (ctas > cap) ctas = cap;
+    cand_sweep_kernel<kWarps><<<ctas, 32 * kWarps, smem, st>>>(a);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st, const WinDesc *wins) {
+                              int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps) {
     if (num_windows == 0) return cudaSuccess;
     SweepArgs a{src, n, window, num_windows, cand, wins};
-    const uint32_t smem = kSweepWarpsPerCta * kHashSize * sizeof(uint16_t);
-    static SmemOnce smem_set_1{0};
-    cudaError_t e = set_smem_once(cand_sweep_kernel, smem, smem_set_1);
-    if (e != cudaSuccess) return e;
-    uint32_t ctas = (num_windows + kSweepWarpsPerCta - 1) / kSweepWarpsPerCta;
-    if (ctas > static_cast<uint32_t>(num_sms)) ctas = num_sms;
-    cand_sweep_kernel<<<ctas, 32 * kSweepWarpsPerCta, smem, st>>>(a);
-    return cudaGetLastError();
+    switch (sweep_warps) {
+    case 4: return launch_sweep_variant<4>(a, num_sms, st);
+    case 5: return launch_sweep_variant<5>(a, num_sms, st);
+    case 6: return launch_sweep_variant<6>(a, num_sms, st);
+    default: return launch_sweep_variant<7>(a, num_sms, st);
+    }
 }
 
 }  // namespace gcz

@@ -46,22 +46,29 @@ namespace gcz {
 namespace {
 
 constexpr uint32_t kMinMatch = 3;                 // MIN_MATCH_LEN, zstd_compress.cu:28
-constexpr uint32_t kSegW = 4096;                  // bytes per speculative segment (one warp)
-constexpr uint32_t kWarps = kMaxWindow / kSegW;   // 16 segments per full window
-constexpr uint32_t kThreads = kWarps * 32;
-// A warp's own parse ends with a step that starts before seg_end and looks at
-// most 127 positions ahead (a wide scan), the lazy step one more; matches do not
-// overlap and are >= 3 bytes, so a list holds at most (kSegW - 1) / 3 + 1
-// entries; lists are written in 32-entry blocks.
-constexpr uint32_t kSpecCap = ((kSegW + 33) / 3 + 1 + 31) / 32 * 32;  // 1408
+// Speculative segment width (bytes per warp) is a schedule knob: 2, 4 or 8 KiB
+// (32, 16 or 8 warps per window).  It never changes the sequences.
+template <uint32_t SegW>
+struct SegCfg {
+    static constexpr uint32_t kSegW = SegW;
+    static constexpr uint32_t kWarps = kMaxWindow / SegW;
+    static constexpr uint32_t kThreads = kWarps * 32;
+    // A warp's own parse ends with a step that starts before seg_end and
+    // looks at most 127 positions ahead (a wide scan), the lazy step one more;
+    // matches do not overlap and are >= 3 bytes, so a list holds at most
+    // (SegW + 127) / 3 + 1 entries; lists are written in 32-entry blocks.
+    static constexpr uint32_t kSpecCap = ((SegW + 128) / 3 + 1 + 31) / 32 * 32;
+    static constexpr uint32_t kLaneCap = kSpecCap + 256;  // + kContCap
+    static constexpr uint32_t kMinBlocks = kThreads >= 1024 ? 1 : 3;
+};
 constexpr uint32_t kContCap = 256;               // continuation matches before giving up
-constexpr uint32_t kLaneCap = kSpecCap + kContCap;
 constexpr uint32_t kNoWarp = 0xFFFFu;
 
 constexpr uint32_t kPre = 64;                           // zero bytes before the window
 constexpr uint32_t kDataBytes = kPre + kMaxWindow + 64; // + zero pad after it
 constexpr uint32_t kBmWords = kMaxWindow / 32 + 8;  // the wide scan reads up to 4 words past a step's first
 
+template <uint32_t kWarps>
 struct SmemLayout {
     uint8_t data[kDataBytes];
     uint32_t bm[kBmWords];  // after the parse, its first kThreads words hold match ends (phase 3)
@@ -78,7 +85,6 @@ struct SmemLayout {
     uint32_t covered;
     alignas(8) uint64_t bar;
 };
-static_assert(kBmWords >= kThreads, "phase 3 reuses the bitmap for match ends");
 
 struct Zstd2Args {
     const uint8_t *src;
@@ -88,13 +94,14 @@ struct Zstd2Args {
     uint32_t num_windows;
     uint32_t lazy;
     uint32_t max_seqs;
-    uint2 *seg;          // per window: kWarps * kLaneCap entries {start | (ml-3)<<16, off}
+    uint2 *seg;          // per window: kWarps * kLaneCap entries {start | (ml-3)<<16, off} (the widest layout's stride)
     uint2 *packed;       // packed output at stride max_seqs (or null)
     uint32_t *ref_seqs;  // reference triples at stride max_seqs (or null)
     uint32_t *seq_counts;
     uint32_t *lit_counts;
     uint32_t *status;
     const WinDesc *wins;
+    uint32_t seg_stride;  // seg entries per window
 };
 
 // ---------------------------------------------------------------- helpers
@@ -404,10 +411,14 @@ struct ListWriter {
 };
 
 // ---------------------------------------------------------------- kernel
-template <bool kRef>
-__global__ void __launch_bounds__(kThreads, 3) zstd_parse_kernel(Zstd2Args a) {
+template <bool kRef, uint32_t SegW>
+__global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBlocks) zstd_parse_kernel(Zstd2Args a) {
+    using C = SegCfg<SegW>;
+    constexpr uint32_t kSegW = C::kSegW, kWarps = C::kWarps, kThreads = C::kThreads;
+    constexpr uint32_t kSpecCap = C::kSpecCap, kLaneCap = C::kLaneCap;
+    static_assert(kBmWords >= kThreads, "phase 3 reuses the bitmap for match ends");
     extern __shared__ __align__(128) uint8_t smem_raw[];
-    SmemLayout &S = *reinterpret_cast<SmemLayout *>(smem_raw);
+    SmemLayout<kWarps> &S = *reinterpret_cast<SmemLayout<kWarps> *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     uint32_t parity = 0;
     if (tid == 0) {
@@ -424,7 +435,7 @@ __global__ void __launch_bounds__(kThreads, 3) zstd_parse_kernel(Zstd2Args a) {
         const uint32_t size =
             a.wins ? a.wins[wi].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
         const uint16_t *cand = a.cand + start;
-        uint2 *seg = a.seg + static_cast<uint64_t>(wi) * kWarps * kLaneCap;
+        uint2 *seg = a.seg + static_cast<uint64_t>(wi) * a.seg_stride;
 
         // ---- 1. stage the window (warp 0), verification bitmap (all warps)
         __syncthreads();  // previous window fully consumed
@@ -662,9 +673,39 @@ __global__ void __launch_bounds__(kThreads, 3) zstd_parse_kernel(Zstd2Args a) {
 
 }  // namespace
 
-size_t zstd2_seg_scratch_entries(uint32_t num_windows) {
-    return static_cast<size_t>(num_windows) * kWarps * kLaneCap;
+// Seg entries per window: the largest of the three layouts, so that a buffer
+// sized once serves every segment width.
+constexpr uint32_t kSegStride = []() constexpr {
+    uint32_t m = SegCfg<2048>::kWarps * SegCfg<2048>::kLaneCap;
+    if (SegCfg<4096>::kWarps * SegCfg<4096>::kLaneCap > m) m = SegCfg<4096>::kWarps * SegCfg<4096>::kLaneCap;
+    if (SegCfg<8192>::kWarps * SegCfg<8192>::kLaneCap > m) m = SegCfg<8192>::kWarps * SegCfg<8192>::kLaneCap;
+    return m;
+}();
+
+size_t zstd2_seg_scratch_entries(uint32_t num_windows) { return static_cast<size_t>(num_windows) * kSegStride; }
+
+namespace {
+template <bool kRef, uint32_t SegW>
+cudaError_t launch_parse_variant(const Zstd2Args &a, int num_sms, int ctas_per_sm, cudaStream_t st) {
+    using C = SegCfg<SegW>;
+    const uint32_t smem = sizeof(SmemLayout<C::kWarps>);
+    static_assert(sizeof(SmemLayout<C::kWarps>) + 1024 <= 233472 / 3, "three CTAs per SM must fit");
+    static SmemOnce smem_set{0};
+    cudaError_t e = set_smem_once(zstd_parse_kernel<kRef, SegW>, smem, smem_set);
+    if (e != cudaSuccess) return e;
+    int grid = num_sms * ctas_per_sm;
+    if (static_cast<uint32_t>(grid) > a.num_windows) grid = static_cast<int>(a.num_windows);
+    zstd_parse_kernel<kRef, SegW><<<grid, C::kThreads, smem, st>>>(a);
+    return cudaGetLastError();
 }
+
+template <bool kRef>
+cudaError_t launch_parse_ref(const Zstd2Args &a, uint32_t seg_width, int num_sms, int ctas_per_sm, cudaStream_t st) {
+    if (seg_width == 2048) return launch_parse_variant<kRef, 2048>(a, num_sms, ctas_per_sm, st);
+    if (seg_width == 8192) return launch_parse_variant<kRef, 8192>(a, num_sms, ctas_per_sm, st);
+    return launch_parse_variant<kRef, 4096>(a, num_sms, ctas_per_sm, st);
+}
+}  // namespace
 
 cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st) {
     if (l.num_windows == 0) return cudaSuccess;
@@ -683,21 +724,9 @@ cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st) {
     a.lit_counts = l.lit_counts;
     a.status = l.status;
     a.wins = l.wins;
-    const uint32_t smem = sizeof(SmemLayout);
-    static_assert(sizeof(SmemLayout) + 1024 <= 233472 / 3, "three CTAs per SM must fit");
-    int grid = l.num_sms * l.ctas_per_sm;
-    if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    cudaError_t e;
-    if (l.ref_seqs) {
-        { static SmemOnce smem_set_1{0}; e = set_smem_once(zstd_parse_kernel<true>, smem, smem_set_1); }
-        if (e != cudaSuccess) return e;
-        zstd_parse_kernel<true><<<grid, kThreads, smem, st>>>(a);
-    } else {
-        { static SmemOnce smem_set_2{0}; e = set_smem_once(zstd_parse_kernel<false>, smem, smem_set_2); }
-        if (e != cudaSuccess) return e;
-        zstd_parse_kernel<false><<<grid, kThreads, smem, st>>>(a);
-    }
-    return cudaGetLastError();
+    a.seg_stride = kSegStride;
+    return l.ref_seqs ? launch_parse_ref<true>(a, l.seg_width, l.num_sms, l.ctas_per_sm, st)
+                      : launch_parse_ref<false>(a, l.seg_width, l.num_sms, l.ctas_per_sm, st);
 }
 
 }  // namespace gcz

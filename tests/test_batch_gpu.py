@@ -97,17 +97,44 @@ def test_zstd_batch_replays_in_cuda_graph(ctx):
     del g
 
 
-def test_autotuner_keeps_results_and_picks_a_config(ctx, tmp_path):
+def _defaults(ctx):
+    for k, v in (("algo", 2), ("parse_ctas", 3), ("staged", 1), ("parse_seg", 4096), ("sweep_warps", 7),
+                 ("lzma_ctas", 3), ("slice_windows", 1024)):
+        ctx.set_option(k, v)
+
+
+def test_autotuner_covers_every_knob_and_keeps_results(ctx, tmp_path, monkeypatch):
+    """Every Zstd schedule (kernel family, sweep warps, segment width, CTAs per
+    SM) gives the same sequences and every LZMA2 schedule the same matches --
+    the tuner checks that as it times them -- and the winners are saved per GPU
+    model and loaded back into a fresh context.  Each timed schedule is also
+    checked against the oracle on a few windows."""
     import gcz
     from gcz import autotune
+    from oracle import oracle as orc
 
-    sample = gcz.gen_synthetic(8, 8 << 20, 8 << 20)
-    out = autotune.tune(ctx, sample, reps=2, save_path=str(tmp_path / "tune.json"))
-    assert out["best"] in [r["config"] for r in out["results"]]
-    assert len(out["results"]) >= 3
-    ctx.set_option("algo", 2)
-    ctx.set_option("parse_ctas", 3)
-    ctx.set_option("staged", 1)
+    monkeypatch.setattr(autotune, "TUNED_DIR", str(tmp_path))
+    z = gcz.gen_synthetic(8, 8 << 20, 8 << 20)
+    lz = gcz.gen_synthetic(9, 8 << 20, 128 << 20)
+    try:
+        out = autotune.tune(ctx, z, lz, reps=1, slices=True)
+        assert len(out["zstd"]["results"]) == len(autotune.ZSTD_CANDIDATES)
+        assert len(out["lzma2"]["results"]) == len(autotune.LZMA_CANDIDATES)
+        assert set(out["best"]) >= {"algo", "lzma_ctas", "slice_windows"}
+        for cfg in autotune.ZSTD_CANDIDATES[::5]:
+            _defaults(ctx)
+            for k, v in cfg.items():
+                ctx.set_option(k, v)
+            s, o = ctx.zstd_match_find(z[:4 * 65536], 16)
+            os_, oo = orc.zstd_sequences(z[:4 * 65536], 16)
+            np.testing.assert_array_equal(o, oo)
+            np.testing.assert_array_equal(s, os_)
+        c2 = gcz.Context(0)
+        assert autotune.apply_tuned(c2) == out["best"]
+        assert all(c2.query(k) == v for k, v in out["best"].items())
+        c2.close()
+    finally:
+        _defaults(ctx)
 
 
 def test_sharded_single_rank_uses_gpu_context(ctx):
