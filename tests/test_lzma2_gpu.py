@@ -90,6 +90,45 @@ def test_against_reference_ptx(ctx):
     np.testing.assert_array_equal(gm, rm)
 
 
+def test_against_reference_ptx_one_pipeline_chunk(ctx):
+    """One reference LZMA2 pipeline chunk (128 MiB, --dict-size 128,
+    pipeline_lzma2.rs:116-190): the reference kernel's 8.5 GiB of slots and
+    counts are reduced on the GPU to the per-position form (first slot,
+    len << 16 | dist, 0 when the count is 0; the reference records at most one
+    match per position) and compared with this library's packed matches
+    there, so nothing large crosses PCIe."""
+    from oracle import ref_kernels
+
+    if not ref_kernels.available():
+        pytest.skip("oracle/_ref not built")
+    import torch as t
+    import gcz
+
+    n = 128 << 20
+    data = gcz.gen_synthetic(3, n, 128 << 20)
+    rk = ref_kernels.RefKernels(0)
+    d_in = rk.to_device(data)
+    bufs = rk.lzma_alloc(n)
+    rk.lzma_launch(d_in, n, bufs)
+    t.cuda.synchronize()
+    m, c = bufs
+    counts = c[:n]
+    assert int(counts.max().item()) <= 1
+    slots = m.view(-1, 8, 2)[:n, 0, :]
+    ref_packed = t.where(counts > 0, (slots[:, 1] << 16) | slots[:, 0], t.zeros_like(counts))
+    del bufs, m, slots
+    t.cuda.empty_cache()
+    B = gcz.num_windows(n)
+    d_packed = t.empty(n, dtype=t.int32, device="cuda")
+    d_has = t.empty(B, dtype=t.uint8, device="cuda")
+    st = t.cuda.current_stream().cuda_stream
+    ctx.lzma2_match_find_device(d_in.data_ptr(), n, 32, d_packed.data_ptr(), d_has.data_ptr(), st)
+    ctx.sync(st)
+    assert t.equal(d_packed, ref_packed)
+    ref_has = (counts.view(B, 65536) > 0).any(dim=1).to(t.uint8)
+    assert t.equal(d_has, ref_has)
+
+
 def test_full_size_1gib_vs_oracle(ctx):
     """LZMA2 L1 workload (1 GiB, seed 3, copy offsets to 128 MiB)."""
     import torch as t
