@@ -1182,7 +1182,7 @@ def run_frames(args):
         "ms_per_step": round(1e3 * sec, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded generator)",
         "config": {"workload": "zstd_l2_frames_1gib", "input_bytes": n, "windows": nb, "slice": "32 MiB, 4 slots",
-                   "entropy_stage": "GPU: Huffman/RLE/raw literals, predefined-FSE sequences, repeat codes",
+                   "entropy_stage": "GPU: Huffman/RLE/raw literals, per-window RLE/FSE-compressed/predefined sequence tables, repeat codes",
                    "compressed_bytes": gpu_bytes, "ratio": round(gpu_bytes / n, 4)},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": n, "d2h_bytes_per_step": gpu_bytes},
         "libzstd_coder_pool": pool,

@@ -218,7 +218,7 @@ class Context:
 
     def zstd_compress_frames_gpu(self, data, level=1):
         """One Zstd frame per 64 KiB window, encoded on the GPU (raw, RLE or
-        Huffman literals; predefined FSE sequence tables): (frames back to back,
+        Huffman literals; RLE, FSE-compressed or predefined sequence tables): (frames back to back,
         frame sizes u64[B])."""
         src = _u8(data)
         n = src.size

@@ -306,12 +306,12 @@ int gcz_zstd_compress_frames(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_
  * GPU block encoder, zstd_compress.cu:756-1038, is unused and its output is
  * not decodable).  Each 64 KiB window becomes one frame with a single block:
  * literals raw, RLE or Huffman-coded (whichever is smallest), sequences
- * FSE-coded with the format's predefined distributions (RFC 8878), repeat
- * offsets used where they apply, or a raw block when that is smaller.  Every
- * frame decodes with stock libzstd to its window.  The frames differ from
- * libzstd's (predefined sequence tables, no tuned ones), so the ratio is a
- * little higher than gcz_zstd_compress_frames' (0.6845 against 0.6775 on the
- * bench data).
+ * FSE-coded (RFC 8878) with, per field and window, an RLE, a normalised
+ * FSE-compressed or the predefined table (whichever an integer size estimate
+ * finds smallest), repeat offsets used where they apply, or a raw block when
+ * that is smaller.  Every frame decodes with stock libzstd to its window.
+ * The frames differ from libzstd's bytes, but their total size is within
+ * 0.1 percentage point of gcz_zstd_compress_frames' on the bench data.
  *
  * gcz_zstd_compress_frames_gpu: host bytes in, frames back to back in `out`
  * (out_capacity >= gcz_zstd_frames_bound(n) always suffices) with
