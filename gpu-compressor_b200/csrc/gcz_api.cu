@@ -205,7 +205,7 @@ size_t nwin(size_t n) { return (n + kW - 1) / kW; }
 // With `wins`, n is the slab size and nbw the number of windows in the table.
 int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, uint32_t depth, void *d_seqs,
                      uint64_t capacity, uint64_t *d_offsets, cudaStream_t st, const gcz::WinDesc *wins = nullptr,
-                     size_t nbw = 0) {
+                     size_t nbw = 0, bool rec8 = false) {
     const size_t nb = wins ? nbw : nwin(n);
     int r;
     if ((r = ensure_dev(c, sc.packed, nb * (size_t)kMaxSeqs * 8)) != GCZ_OK) return r;
@@ -256,8 +256,12 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
         c->all_launches += 1;
     }
     GCZ_CUDA(c, gcz::launch_scan_counts(counts, (uint32_t)nb, d_offsets, st));
-    GCZ_CUDA(c, gcz::launch_expand_seqs(sc.packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
-                                        c->d_status, c->num_sms, st));
+    if (rec8)
+        GCZ_CUDA(c, gcz::launch_compact_seqs(sc.packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
+                                             c->d_status, c->num_sms, st));
+    else
+        GCZ_CUDA(c, gcz::launch_expand_seqs(sc.packed.p, counts, d_offsets, (uint32_t)nb, kMaxSeqs, d_seqs, capacity,
+                                            c->d_status, c->num_sms, st));
     c->all_launches += 2;
     return GCZ_OK;
 }
@@ -559,7 +563,8 @@ extern "C" int gcz_zstd_match_find_device(gcz_ctx *c, const uint8_t *d_src, size
 namespace {
 // Second half of a Zstd pipeline slice: wait for its offsets, then queue the
 // copy of its sequences into the caller's array.
-int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, uint64_t *offsets, uint64_t &done) {
+int zstd_finish_slot(gcz_ctx *c, Slot &sl, void *seqs, size_t cap, uint64_t *offsets, uint64_t &done,
+                     uint32_t rec_bytes) {
     GCZ_CUDA(c, cudaEventSynchronize(sl.ev));
     const uint64_t *ho = static_cast<const uint64_t *>(sl.h_off.p);
     const uint64_t total = ho[sl.sb];
@@ -567,7 +572,9 @@ int zstd_finish_slot(gcz_ctx *c, Slot &sl, gcz_zstd_sequence *seqs, size_t cap, 
     if (done + total > cap)
         return fail(c, GCZ_ECAPACITY, "need %llu sequences, capacity %zu", (unsigned long long)(done + total), cap);
     // On the copy-out stream, so that the slot's next copy-in does not queue behind it.
-    if (total) GCZ_CUDA(c, cudaMemcpyAsync(seqs + done, sl.seqs.p, total * 16, cudaMemcpyDeviceToHost, c->out_stream));
+    if (total)
+        GCZ_CUDA(c, cudaMemcpyAsync(static_cast<uint8_t *>(seqs) + done * rec_bytes, sl.seqs.p, total * rec_bytes,
+                                    cudaMemcpyDeviceToHost, c->out_stream));
     GCZ_CUDA(c, cudaEventRecord(sl.ev_out, c->out_stream));
     for (size_t i = 1; i <= sl.sb; i++) offsets[sl.b0 + i] = done + ho[i];
     done += total;
@@ -598,11 +605,11 @@ int drain_slots(gcz_ctx *c) {
 // queues its copy-out, so the host's wait never holds back the next copy-in
 // (two slots, finishing slice k-1: 47.7 GB/s for 1 GiB; four: 48.8, against
 // 51.8 for the same copies with no kernels).
-extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
-                                   gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets) {
-    if (!c) return GCZ_EINVAL;
-    std::lock_guard<std::mutex> lk(c->mu);
-    if ((n && (!src || !seqs)) || !offsets) return fail(c, GCZ_EINVAL, "null pointer");
+namespace {
+// The host-buffer Zstd pipeline: records of rec_bytes (16: ZSTD_Sequence, 8:
+// packed {ll | (ml-3) << 16, off}) back to back in `seqs`.
+int zstd_host_pipeline(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth, void *seqs,
+                       size_t seq_capacity, uint64_t *offsets, uint32_t rec_bytes) {
     DeviceGuard g(c->device);
     const size_t nb = nwin(n);
     offsets[0] = 0;
@@ -625,23 +632,41 @@ extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uin
         GCZ_CUDA(c, cudaMemcpyAsync(sl.in.p, src + sl.off, sl.len, cudaMemcpyHostToDevice, sl.st));
         GCZ_CUDA(c, cudaStreamWaitEvent(sl.st, sl.ev_out, 0));  // sl.seqs free again
         if ((r = zstd_device_core(c, sl.sc, static_cast<const uint8_t *>(sl.in.p), sl.len, search_depth, sl.seqs.p,
-                                  slice_cap, static_cast<uint64_t *>(sl.offsets.p), sl.st)) != GCZ_OK)
+                                  slice_cap, static_cast<uint64_t *>(sl.offsets.p), sl.st, nullptr, 0,
+                                  rec_bytes == 8)) != GCZ_OK)
             break;
         GCZ_CUDA(c, cudaMemcpyAsync(sl.h_off.p, sl.offsets.p, (sb + 1) * 8, cudaMemcpyDeviceToHost, sl.st));
         GCZ_CUDA(c, cudaEventRecord(sl.ev, sl.st));
         sl.busy = true;
         if (k >= kS - 1) {  // finish slice k-(S-1); slices finish in order, so records stay in order
             Slot &old = c->slots[(k - (kS - 1)) % kS];
-            if (old.busy) r = zstd_finish_slot(c, old, seqs, seq_capacity, offsets, done);
+            if (old.busy) r = zstd_finish_slot(c, old, seqs, seq_capacity, offsets, done, rec_bytes);
         }
     }
     for (size_t j = k >= kS - 1 ? k - (kS - 1) : 0; j < k && r == GCZ_OK; ++j) {
         Slot &rest = c->slots[j % kS];
-        if (rest.busy) r = zstd_finish_slot(c, rest, seqs, seq_capacity, offsets, done);
+        if (rest.busy) r = zstd_finish_slot(c, rest, seqs, seq_capacity, offsets, done, rec_bytes);
     }
     for (Slot &sl : c->slots) sl.busy = false;
     const int r2 = drain_slots(c);
     return r != GCZ_OK ? r : r2;
+}
+}  // namespace
+
+extern "C" int gcz_zstd_match_find(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
+                                   gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!src || !seqs)) || !offsets) return fail(c, GCZ_EINVAL, "null pointer");
+    return zstd_host_pipeline(c, src, n, search_depth, seqs, seq_capacity, offsets, 16);
+}
+
+extern "C" int gcz_zstd_match_find_packed(gcz_ctx *c, const uint8_t *src, size_t n, uint32_t search_depth,
+                                          uint64_t *records, size_t record_capacity, uint64_t *offsets) {
+    if (!c) return GCZ_EINVAL;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((n && (!src || !records)) || !offsets) return fail(c, GCZ_EINVAL, "null pointer");
+    return zstd_host_pipeline(c, src, n, search_depth, records, record_capacity, offsets, 8);
 }
 
 extern "C" int gcz_zstd_encode_frames_device(gcz_ctx *c, const uint8_t *d_src, size_t n,

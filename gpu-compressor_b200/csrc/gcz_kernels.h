@@ -80,6 +80,10 @@ cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *o
 cudaError_t launch_expand_seqs(const void *packed, const uint32_t *counts, const uint64_t *offsets, uint32_t num,
                                uint32_t max_seqs, void *out, uint64_t capacity, uint32_t *status, int num_sms,
                                cudaStream_t st);
+// 8-byte records {ll | (ml-3) << 16, off} instead of ZSTD_Sequence.
+cudaError_t launch_compact_seqs(const void *packed, const uint32_t *counts, const uint64_t *offsets, uint32_t num,
+                                uint32_t max_seqs, void *out, uint64_t capacity, uint32_t *status, int num_sms,
+                                cudaStream_t st);
 cudaError_t launch_zstd_literals(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows,
                                  const uint32_t *ref_seqs, const uint32_t *seq_counts, uint32_t max_seqs, uint8_t *lits,
                                  int num_sms, cudaStream_t st);

@@ -310,6 +310,23 @@ __global__ void __launch_bounds__(256) expand_seqs_kernel(const uint2 *packed, c
     }
 }
 
+// The same records compacted as 8 bytes each: {litLength | (matchLength-3) << 16,
+// offset} (a window's lengths and offsets are below 65536).
+__global__ void __launch_bounds__(256) compact_seqs_kernel(const uint2 *packed, const uint32_t *counts,
+                                                           const uint64_t *offsets, uint32_t num, uint32_t max_seqs,
+                                                           uint2 *out, uint64_t capacity, uint32_t *status) {
+    for (uint32_t w = blockIdx.x; w < num; w += gridDim.x) {
+        const uint32_t cnt = counts[w];
+        const uint64_t o = offsets[w];
+        const uint2 *src = packed + static_cast<uint64_t>(w) * max_seqs;
+        if (o + cnt > capacity) {
+            if (threadIdx.x == 0) atomicOr(status, kErrCapacity);
+            continue;
+        }
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) out[o + i] = src[i];
+    }
+}
+
 // Literal bytes in the reference layout (zstd_compress.cu:311-314,341-343):
 // every byte not covered by a match, in order, at stride `window` per window.
 // One warp per window walks its sequences.
@@ -403,6 +420,17 @@ cudaError_t launch_expand_seqs(const void *packed, const uint32_t *counts, const
     if (static_cast<uint32_t>(grid) > num) grid = static_cast<int>(num);
     expand_seqs_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const uint2 *>(packed), counts, offsets, num, max_seqs,
                                              reinterpret_cast<uint4 *>(out), capacity, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_seqs(const void *packed, const uint32_t *counts, const uint64_t *offsets, uint32_t num,
+                                uint32_t max_seqs, void *out, uint64_t capacity, uint32_t *status, int num_sms,
+                                cudaStream_t st) {
+    if (num == 0) return cudaSuccess;
+    int grid = num_sms * 8;
+    if (static_cast<uint32_t>(grid) > num) grid = static_cast<int>(num);
+    compact_seqs_kernel<<<grid, 256, 0, st>>>(reinterpret_cast<const uint2 *>(packed), counts, offsets, num, max_seqs,
+                                              reinterpret_cast<uint2 *>(out), capacity, status);
     return cudaGetLastError();
 }
 

@@ -122,6 +122,18 @@ class Context:
                                           offsets.ctypes.data))
         return seqs[:int(offsets[-1])], offsets
 
+    def zstd_match_find_packed(self, data, search_depth=16):
+        """8-byte records u64[N] (litLength | (matchLength-3) << 16 | offset << 32)
+        and per-window offsets u64[B+1]; expand_packed() gives ZSTD_Sequence records."""
+        src = _u8(data)
+        n = src.size
+        cap = int(L.gcz_zstd_max_sequences(n))
+        recs = np.empty(max(cap, 1), np.uint64)
+        offsets = np.zeros(num_windows(n) + 1, np.uint64)
+        self._check(L.gcz_zstd_match_find_packed(self._h, _ptr(src), n, search_depth, recs.ctypes.data, cap,
+                                                 offsets.ctypes.data))
+        return recs[:int(offsets[-1])], offsets
+
     def zstd_match_find_device(self, d_src, n, search_depth, d_seqs, capacity, d_offsets, stream=None):
         """Device pointers (ints); enqueue only."""
         self._check(L.gcz_zstd_match_find_device(self._h, d_src, n, search_depth, d_seqs, capacity, d_offsets,
@@ -347,6 +359,17 @@ def gen_synthetic(seed, n, max_offset=8 << 20, mix=(0.4, 0.4, 0.2), out=None):
         out = np.empty(n, np.uint8)
     if n:
         L.gcz_gen_synthetic(seed, out.ctypes.data, n, max_offset, float(mix[0]), float(mix[1]), float(mix[2]))
+    return out
+
+
+def expand_packed(records):
+    """ZSTD_Sequence records u32[N, 4] (offset, litLength, matchLength, rep = 0)
+    from gcz_zstd_match_find_packed's 8-byte records: the caller-side loop."""
+    r = np.asarray(records, dtype=np.uint64)
+    out = np.zeros((r.size, 4), np.uint32)
+    out[:, 0] = (r >> np.uint64(32)).astype(np.uint32)
+    out[:, 1] = (r & np.uint64(0xFFFF)).astype(np.uint32)
+    out[:, 2] = ((r >> np.uint64(16)) & np.uint64(0xFFFF)).astype(np.uint32) + 3
     return out
 
 

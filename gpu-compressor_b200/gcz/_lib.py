@@ -42,6 +42,7 @@ SIGNATURES = {
     "gcz_num_windows": (_sz, [_sz]),
     "gcz_zstd_max_sequences": (_sz, [_sz]),
     "gcz_zstd_match_find": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp]),
+    "gcz_zstd_match_find_packed": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp]),
     "gcz_zstd_match_find_device": (_i, [_vp, _vp, _sz, _u32, _vp, _sz, _vp, _vp]),
     "gcz_zstd_match_find_device_noalloc": (_i, [_i, _vp, _sz, _u32, _vp, _sz, _vp, _vp]),
     "gcz_zstd_match_find_ref_layout_device": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _u32, _u32, _u32, _u32, _u32, _vp]),

@@ -113,6 +113,16 @@ size_t gcz_zstd_max_sequences(size_t n);
 int gcz_zstd_match_find(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t search_depth,
                         gcz_zstd_sequence *seqs, size_t seq_capacity, uint64_t *offsets);
 
+/* No counterpart in the reference.  gcz_zstd_match_find with 8-byte records
+ * instead of 16-byte ZSTD_Sequence: record i = litLength | (matchLength - 3) << 16
+ * | (uint64_t)offset << 32 (a 64 KiB window's lengths and offsets fit 16 bits).
+ * Half the bytes cross PCIe back, next to the input going in; the caller
+ * expands each record to ZSTD_Sequence{offset, litLength, matchLength, 0}
+ * before ZSTD_compressSequences (a loop in INTEGRATION.md).  Offsets and
+ * order as gcz_zstd_match_find. */
+int gcz_zstd_match_find_packed(gcz_ctx *ctx, const uint8_t *src, size_t n, uint32_t search_depth, uint64_t *records,
+                               size_t record_capacity, uint64_t *window_offsets);
+
 /* Same on device memory.  d_src must be 16-byte aligned.  d_seqs needs
  * gcz_zstd_max_sequences(n) entries (or the actual count), d_offsets
  * num_windows+1 entries.  Enqueued on `stream` (cudaStream_t; NULL = the

@@ -171,3 +171,17 @@ def test_loaded_kernel_image_is_sm100(ctx):
     """The kernels the runtime loaded from libgcz.so were compiled for sm_100a
     (binaryVersion 100 from cudaFuncGetAttributes), not JIT-compiled from PTX."""
     assert ctx.query("binary_version") == 100
+
+
+def test_packed_records_expand_to_the_sequences(ctx):
+    """gcz_zstd_match_find_packed's 8-byte records expand (caller-side) to
+    exactly gcz_zstd_match_find's ZSTD_Sequence records, with the same window
+    offsets, across the host pipeline's slices."""
+    import gcz
+
+    for seed, n in ((61, 5 * 65536 + 77), (62, 70 << 20)):
+        data = gcz.gen_synthetic(seed, n, 8 << 20)
+        s, o = ctx.zstd_match_find(data, 64)
+        r, o2 = ctx.zstd_match_find_packed(data, 64)
+        np.testing.assert_array_equal(o2, o)
+        np.testing.assert_array_equal(gcz.expand_packed(r), s)

@@ -53,6 +53,12 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls():
         total = int(w_off[-1])
         assert total > 0
         np.testing.assert_array_equal(got_seqs[:total].cpu().numpy(), want_seqs[:total].cpu().numpy())
+        if call == 1:  # and, directly, the oracle (the CPU restatement pinned to the reference kernels)
+            from oracle import oracle as orc
+
+            o_seqs, o_off = orc.zstd_sequences(data, 16)
+            np.testing.assert_array_equal(got_off.cpu().numpy().astype(np.uint64), o_off)
+            np.testing.assert_array_equal(got_seqs[:total].cpu().numpy().view(np.uint32), o_seqs)
         del want_seqs, got_seqs
     ctx.close()
 
