@@ -268,17 +268,26 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
         uint32_t *rm = a.ref_matches ? a.ref_matches + start * a.max_matches * 2u : nullptr;
         uint32_t any = 0;
         const uint32_t nsteps = (size + 31u) >> 5;
+        // Each warp takes a contiguous range of steps, so a run of matches
+        // (cand(q) = cand(q-1) + 1) carries from one step's last lane into the
+        // next step's first: lane 0 then derives its length instead of
+        // extending again.  The carried length is exact when it is below 273
+        // (an extension is cut only at 273 + 31 bytes or at the window's end).
+        constexpr uint32_t kL2Warps = kL2Threads / 32;
+        const uint32_t per = (nsteps + kL2Warps - 1u) / kL2Warps;
+        const uint32_t s_begin = warp * per, s_end = min(nsteps, s_begin + per);
+        uint32_t carry_c = kNone, carry_e = 0;  // last lane of the previous step: candidate, length (0: none)
         // The next step's candidates are loaded while this step is verified.
-        uint32_t c_next = (warp < nsteps && warp * 32u + lane + 3u < size) ? cand[warp * 32u + lane] : kNone;
-        for (uint32_t st = warp; st < nsteps; st += kL2Threads / 32) {
+        uint32_t c_next = (s_begin < s_end && s_begin * 32u + lane + 3u < size) ? cand[s_begin * 32u + lane] : kNone;
+        for (uint32_t st = s_begin; st < s_end; ++st) {
             const uint32_t q = st * 32u + lane;
             const bool inwin = q < size;
             const bool valid4 = q + 3u < size;
             const uint32_t x = win.u32(q);
             const uint32_t c = valid4 ? c_next : kNone;
             {
-                const uint32_t st2 = st + kL2Threads / 32, q2 = st2 * 32u + lane;
-                c_next = (st2 < nsteps && q2 + 3u < size) ? static_cast<uint32_t>(cand[q2]) : kNone;
+                const uint32_t st2 = st + 1u, q2 = st2 * 32u + lane;
+                c_next = (st2 < s_end && q2 + 3u < size) ? static_cast<uint32_t>(cand[q2]) : kNone;
             }
             const bool has = valid4 && a.search_depth > 0 && c != kNone;
             const uint32_t y = has ? win.u32(c) : ~x;
@@ -296,9 +305,13 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
             const uint32_t bound = size - q < kLzmaMaxMatch + 31u ? size - q : kLzmaMaxMatch + 31u;
             bool pending = false;
             if (eq4 && !cont) {
-                const uint32_t lim1 = bound < 20u ? bound : 20u;
-                ext = extend_lane(win, c, q, 4u, lim1);
-                pending = ext == lim1 && lim1 < bound;
+                if (lane == 0 && carry_e > 4u && carry_e < kLzmaMaxMatch && c == carry_c + 1u) {
+                    ext = carry_e - 1u;  // the previous step's last match, one byte on
+                } else {
+                    const uint32_t lim1 = bound < 20u ? bound : 20u;
+                    ext = extend_lane(win, c, q, 4u, lim1);
+                    pending = ext == lim1 && lim1 < bound;
+                }
             }
             for (uint32_t pend = __ballot_sync(kFull, pending); pend; pend &= pend - 1u) {
                 const uint32_t hl = static_cast<uint32_t>(__ffs(pend)) - 1u;
@@ -323,6 +336,11 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
                 if (lane == hl) ext = len2;
             }
             const uint32_t ext_head = __shfl_sync(kFull, ext, head);
+            {
+                const uint32_t e31 = eq4 ? ext_head - (lane - head) : 0u;
+                carry_e = __shfl_sync(kFull, e31, 31);
+                carry_c = __shfl_sync(kFull, c, 31);
+            }
             uint32_t dist = 0, len = 0;
             if (inwin && q + 1u < size) {
                 if (eq4) {
