@@ -46,39 +46,43 @@ namespace gcz {
 namespace {
 
 constexpr uint32_t kMinMatch = 3;                 // MIN_MATCH_LEN, zstd_compress.cu:28
-// Speculative segment width (bytes per warp) is a schedule knob: 2, 4 or 8 KiB
-// (32, 16 or 8 warps per window).  It never changes the sequences.
-template <uint32_t SegW>
+// Speculative segment width is a schedule knob: 2, 4 or 8 KiB parsed by one
+// warp each (32, 16 or 8 warps per window), or 1 KiB parsed by an 8-lane group
+// (four segments per warp, 64 per window).  It never changes the sequences.
+template <uint32_t SegW, uint32_t GL = 32>
 struct SegCfg {
     static constexpr uint32_t kSegW = SegW;
-    static constexpr uint32_t kWarps = kMaxWindow / SegW;
-    static constexpr uint32_t kThreads = kWarps * 32;
-    // A warp's own parse ends with a step that starts before seg_end and
-    // looks at most 127 positions ahead (a wide scan), the lazy step one more;
-    // matches do not overlap and are >= 3 bytes, so a list holds at most
-    // (SegW + 127) / 3 + 1 entries; lists are written in 32-entry blocks.
-    static constexpr uint32_t kSpecCap = ((SegW + 128) / 3 + 1 + 31) / 32 * 32;
-    static constexpr uint32_t kLaneCap = kSpecCap + 256;  // + kContCap
+    static constexpr uint32_t kSegs = kMaxWindow / SegW;
+    static constexpr uint32_t kThreads = kSegs * GL;
+    static constexpr uint32_t kWarps = kThreads / 32;
+    // A segment's own parse ends with a step that starts before seg_end and
+    // looks at most kLook positions ahead (a warp's wide scan 128, a group's
+    // scan 32), the lazy step one more; matches do not overlap and are >= 3
+    // bytes, so a list holds at most (SegW + kLook) / 3 + 1 entries; lists are
+    // written in 32-entry blocks.
+    static constexpr uint32_t kLook = GL == 32 ? 128 : 32;
+    static constexpr uint32_t kSpecCap = ((SegW + kLook) / 3 + 1 + 31) / 32 * 32;
+    static constexpr uint32_t kContCap = GL == 32 ? 256 : 128;  // continuation matches before giving up
+    static constexpr uint32_t kLaneCap = kSpecCap + kContCap;
     static constexpr uint32_t kMinBlocks = kThreads >= 1024 ? 1 : 3;
 };
-constexpr uint32_t kContCap = 256;               // continuation matches before giving up
 constexpr uint32_t kNoWarp = 0xFFFFu;
 
 constexpr uint32_t kPre = 64;                           // zero bytes before the window
 constexpr uint32_t kDataBytes = kPre + kMaxWindow + 64; // + zero pad after it
 constexpr uint32_t kBmWords = kMaxWindow / 32 + 8;  // the wide scan reads up to 4 words past a step's first
 
-template <uint32_t kWarps>
+template <uint32_t kSegs>
 struct SmemLayout {
     uint8_t data[kDataBytes];
     uint32_t bm[kBmWords];  // after the parse, its first kThreads words hold match ends (phase 3)
-    uint32_t spec_count[kWarps];
-    uint32_t cont_count[kWarps];
-    uint32_t sync_warp[kWarps];
-    uint32_t sync_idx[kWarps];
-    uint32_t chain_from[kWarps];
-    uint32_t out_off[kWarps];
-    uint32_t on_chain[kWarps];
+    uint32_t spec_count[kSegs];
+    uint32_t cont_count[kSegs];
+    uint32_t sync_warp[kSegs];
+    uint32_t sync_idx[kSegs];
+    uint32_t chain_from[kSegs];
+    uint32_t out_off[kSegs];
+    uint32_t on_chain[kSegs];
     uint32_t carry;
     uint32_t flags;
     uint32_t total;
@@ -94,7 +98,7 @@ struct Zstd2Args {
     uint32_t num_windows;
     uint32_t lazy;
     uint32_t max_seqs;
-    uint2 *seg;          // per window: kWarps * kLaneCap entries {start | (ml-3)<<16, off} (the widest layout's stride)
+    uint2 *seg;          // per window: kSegs * kLaneCap entries {start | (ml-3)<<16, off} (the widest layout's stride)
     uint2 *packed;       // packed output at stride max_seqs (or null)
     uint32_t *ref_seqs;  // reference triples at stride max_seqs (or null)
     uint32_t *seq_counts;
@@ -383,6 +387,123 @@ __device__ __forceinline__ bool warp_step(const Win &w, const uint32_t *bm, Cand
     return true;
 }
 
+// Group-wide extension: the lanes of each GL-lane group compare 4 bytes each
+// (4 * GL per iteration) of their group's own (c, q, lim) and get the first
+// index in [0, lim) where bytes c+i and q+i differ, else lim; groups with
+// act == false get 0.  All 32 lanes call it (the loop runs while any group
+// is still extending).
+template <uint32_t GL>
+__device__ __forceinline__ uint32_t extend_group(const Win &w, uint32_t c, uint32_t q, uint32_t lim, bool act) {
+    const uint32_t lane = lane_id(), gl = lane & (GL - 1u), gb = lane & ~(GL - 1u);
+    uint32_t len = 0, out = 0;
+    bool done = !act;
+    while (__any_sync(kFull, !done)) {
+        const uint32_t k = len + 4u * gl;
+        uint32_t res = k;
+        if (!done && k < lim) {
+            const uint32_t d = w.u32(static_cast<int>(q + k)) ^ w.u32(static_cast<int>(c + k));
+            const uint32_t fb = d ? (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3 : 4u;
+            const uint32_t rem = lim - k;
+            res = k + (fb < rem ? fb : rem);
+        }
+        const uint32_t sb = (__ballot_sync(kFull, !done && res < k + 4u) >> gb) & ((1u << GL) - 1u);
+        const uint32_t v = __shfl_sync(kFull, res, gb + (sb ? static_cast<uint32_t>(__ffs(sb)) - 1u : 0u));
+        if (!done && sb) {
+            out = v;
+            done = true;
+        }
+        len += 4u * GL;
+    }
+    return out;
+}
+
+// One step of the exact parse for every 8-lane group of the warp at once,
+// each from its own state s (group-uniform); groups with run == false keep
+// theirs.  A group looks at the 32 positions from s.p: the hash-match bits
+// come from the bitmap, and each lane tests the three repeat offsets on four
+// positions (8-byte compares) among those before the first hash match
+// (zstd_compress.cu:259-275).  The first event is the match, extended 32
+// bytes per group iteration, with the lazy step (:278-307) at f+1; with no
+// event the group moves over the 32 positions.  Returns whether the group
+// found a match (m set, s advanced past it, repeat offsets updated).
+__device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, const uint16_t *cand, uint32_t size,
+                                           bool lazy, bool run, PState &s, Match &m) {
+    constexpr uint32_t GL = 8;
+    const uint32_t lane = lane_id(), gl = lane & (GL - 1u), gb = lane & ~(GL - 1u);
+    const uint32_t p = run ? s.p : 0u;
+    const uint32_t lim = run ? size - 3u - p : 0u;
+    const uint32_t n32 = lim < 32u ? lim : 32u;
+    uint32_t H = __funnelshift_r(bm[p >> 5], bm[(p >> 5) + 1], p & 31u);
+    if (n32 < 32u) H &= (1u << n32) - 1u;
+    const uint32_t nh = H ? static_cast<uint32_t>(__ffs(H)) - 1u : n32;  // positions without a hash match
+    const uint32_t j0 = 4u * gl;
+    const uint32_t q0 = j0 < nh ? p + j0 : p;
+    const uint32_t vlim = j0 < nh ? (nh - j0 < 4u ? nh - j0 : 4u) : 0u;  // positions of this lane to test
+    const uint32_t xlo = w.u32(static_cast<int>(q0)), xhi = w.u32(static_cast<int>(q0 + 4u));
+    uint32_t mk[3];
+#pragma unroll
+    for (uint32_t k = 0; k < 3; ++k) {
+        const uint32_t rv = k == 0u ? s.r0 : (k == 1u ? s.r1 : s.r2);
+        // positions q0 + t with t < vlim and q0 + t >= rv; their source bytes start at q0 - rv + t >= 0
+        const uint32_t tmin = rv > q0 ? rv - q0 : 0u;
+        const uint32_t valid = tmin < vlim ? ((1u << vlim) - 1u) & ~((1u << tmin) - 1u) : 0u;
+        const int yb = valid ? static_cast<int>(q0) - static_cast<int>(rv) : static_cast<int>(q0);
+        const uint32_t dlo = xlo ^ w.u32(yb), dhi = xhi ^ w.u32(yb + 4);
+        const uint32_t e = ((dlo & 0xFFFFFFu) == 0u ? 1u : 0u) | ((dlo >> 8) == 0u ? 2u : 0u) |
+                           ((__funnelshift_r(dlo, dhi, 16) & 0xFFFFFFu) == 0u ? 4u : 0u) |
+                           ((__funnelshift_r(dlo, dhi, 24) & 0xFFFFFFu) == 0u ? 8u : 0u);
+        mk[k] = e & valid;
+    }
+    const uint32_t any = mk[0] | mk[1] | mk[2];
+    const uint32_t rb = (__ballot_sync(kFull, any != 0u) >> gb) & 0xFFu;
+    const uint32_t l = rb ? static_cast<uint32_t>(__ffs(rb)) - 1u : 0u;
+    const uint32_t al = __shfl_sync(kFull, any, gb + l), m0 = __shfl_sync(kFull, mk[0], gb + l),
+                   m1 = __shfl_sync(kFull, mk[1], gb + l);
+    const bool rep = rb != 0u;
+    const bool ev = run && (rep || nh < n32);
+    uint32_t f = p + nh, r = 0;
+    if (rep) {
+        const uint32_t t = static_cast<uint32_t>(__ffs(al)) - 1u;
+        f = p + 4u * l + t;
+        r = (m0 >> t) & 1u ? 0u : ((m1 >> t) & 1u ? 1u : 2u);
+    }
+    const uint32_t fc = ev ? f : 0u;
+    const uint32_t cf = zmap(cand[fc]), cf1 = zmap(cand[fc + 1u]);
+    uint32_t off, c0;
+    if (!rep) {
+        off = fc - cf;
+        c0 = cf;
+    } else {  // first repeat offset with 3 equal bytes wins
+        off = r == 0u ? s.r0 : (r == 1u ? s.r1 : s.r2);
+        c0 = fc - off;
+    }
+    // The lazy candidate at f+1 is skipped when it is the same match one byte on
+    // (cand(f+1) == c0 + 1): it is exactly one byte shorter, never taken.
+    const bool ltry = ev && lazy && fc + 4u < size && bm_bit(bm, fc + 1u) && cf1 != c0 + 1u;
+    const uint32_t e1 = extend_group<GL>(w, c0 + kMinMatch, fc + kMinMatch, ev ? size - fc - kMinMatch : 0u, ev);
+    const uint32_t e2 =
+        extend_group<GL>(w, cf1 + kMinMatch, fc + 1u + kMinMatch, ltry ? size - fc - 1u - kMinMatch : 0u, ltry);
+    uint32_t len = e1 + kMinMatch;
+    f = fc;
+    if (ltry && e2 + kMinMatch > len + 1u) {
+        f = fc + 1u;
+        len = e2 + kMinMatch;
+        off = f - cf1;
+    }
+    if (ev) {
+        m.start = f;
+        m.len = len;
+        m.off = off;
+        s.r2 = s.r1;
+        s.r1 = s.r0;
+        s.r0 = off;
+        s.p = f + len;
+    } else if (run) {
+        s.p = p + n32;
+    }
+    return ev;
+}
+
 __device__ __forceinline__ uint2 pack_entry(const Match &m) {
     return make_uint2(m.start | ((m.len - kMinMatch) << 16), m.off);
 }
@@ -411,14 +532,15 @@ struct ListWriter {
 };
 
 // ---------------------------------------------------------------- kernel
-template <bool kRef, uint32_t SegW>
-__global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBlocks) zstd_parse_kernel(Zstd2Args a) {
-    using C = SegCfg<SegW>;
-    constexpr uint32_t kSegW = C::kSegW, kWarps = C::kWarps, kThreads = C::kThreads;
-    constexpr uint32_t kSpecCap = C::kSpecCap, kLaneCap = C::kLaneCap;
+template <bool kRef, uint32_t SegW, uint32_t GL>
+__global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::kMinBlocks)
+    zstd_parse_kernel(Zstd2Args a) {
+    using C = SegCfg<SegW, GL>;
+    constexpr uint32_t kSegW = C::kSegW, kWarps = C::kWarps, kThreads = C::kThreads, kSegs = C::kSegs;
+    constexpr uint32_t kSpecCap = C::kSpecCap, kLaneCap = C::kLaneCap, kContCap = C::kContCap;
     static_assert(kBmWords >= kThreads, "phase 3 reuses the bitmap for match ends");
     extern __shared__ __align__(128) uint8_t smem_raw[];
-    SmemLayout<kWarps> &S = *reinterpret_cast<SmemLayout<kWarps> *>(smem_raw);
+    SmemLayout<kSegs> &S = *reinterpret_cast<SmemLayout<kSegs> *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     uint32_t parity = 0;
     if (tid == 0) {
@@ -480,55 +602,148 @@ __global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBloc
         }
         __syncthreads();
 
-        // ---- 2a. speculative parse of each segment (one warp each)
         const uint32_t lim_pos = size > 3u ? size - 3u : 0u;  // positions q < lim_pos can start a match
-        const uint32_t seg_start = warp * kSegW, seg_end = seg_start + kSegW;
-        const bool active = seg_start < lim_pos;
-        const bool last_active = !(seg_end < lim_pos);
-        ListWriter lw(seg + warp * kLaneCap);
-        PState s{seg_start, 1u, 4u, 8u};
-        CandBuf cb{cand, size, 0u, 0u, 0u, 0u};
-        if (active) cb.init(seg_start);
-        if (active) {
-            const uint32_t stop = last_active ? size : seg_end;
-            Match m;
-            while (s.p < stop && s.p + 3u < size) {
-                if (warp_step(win, S.bm, cb, size, lazy, s, m)) lw.put(pack_entry(m));
-            }
-            lw.flush();
-        }
-        if (lane == 0) {
-            S.spec_count[warp] = lw.n;
-            S.cont_count[warp] = 0;
-            S.sync_warp[warp] = kNoWarp;
-            S.sync_idx[warp] = 0;
-        }
-        __syncthreads();
-
-        // ---- 2b. continue each warp's parse until it meets a later warp's list
-        if (active && !last_active) {
-            ListWriter cw(seg + warp * kLaneCap + kSpecCap);
-            uint32_t t = kNoWarp, j = 0;
-            Match m;
-            while (s.p + 3u < size) {
-                if (!warp_step(win, S.bm, cb, size, lazy, s, m)) continue;
-                const uint32_t tw = m.start / kSegW;  // warp whose segment holds this match start
-                if (tw != t) {
-                    t = tw;
-                    j = 0;
+        if constexpr (GL == 32) {
+            // ---- 2a. speculative parse of each segment (one warp each)
+            const uint32_t seg_start = warp * kSegW, seg_end = seg_start + kSegW;
+            const bool active = seg_start < lim_pos;
+            const bool last_active = !(seg_end < lim_pos);
+            ListWriter lw(seg + warp * kLaneCap);
+            PState s{seg_start, 1u, 4u, 8u};
+            CandBuf cb{cand, size, 0u, 0u, 0u, 0u};
+            if (active) cb.init(seg_start);
+            if (active) {
+                const uint32_t stop = last_active ? size : seg_end;
+                Match m;
+                while (s.p < stop && s.p + 3u < size) {
+                    if (warp_step(win, S.bm, cb, size, lazy, s, m)) lw.put(pack_entry(m));
                 }
-                const uint32_t tcount = S.spec_count[t];
-                const uint2 *tl = seg + t * kLaneCap;
-                // first entry of t's list with start >= m.start (lists are sorted by start)
-                for (;;) {
-                    const uint32_t idx = j + lane;
-                    const bool ge = idx >= tcount || (tl[idx].x & 0xFFFFu) >= m.start;
-                    const uint32_t b = __ballot_sync(kFull, ge);
-                    if (b) {
-                        j += static_cast<uint32_t>(__ffs(b)) - 1u;
+                lw.flush();
+            }
+            if (lane == 0) {
+                S.spec_count[warp] = lw.n;
+                S.cont_count[warp] = 0;
+                S.sync_warp[warp] = kNoWarp;
+                S.sync_idx[warp] = 0;
+            }
+            __syncthreads();
+
+            // ---- 2b. continue each warp's parse until it meets a later warp's list
+            if (active && !last_active) {
+                ListWriter cw(seg + warp * kLaneCap + kSpecCap);
+                uint32_t t = kNoWarp, j = 0;
+                Match m;
+                while (s.p + 3u < size) {
+                    if (!warp_step(win, S.bm, cb, size, lazy, s, m)) continue;
+                    const uint32_t tw = m.start / kSegW;  // warp whose segment holds this match start
+                    if (tw != t) {
+                        t = tw;
+                        j = 0;
+                    }
+                    const uint32_t tcount = S.spec_count[t];
+                    const uint2 *tl = seg + t * kLaneCap;
+                    // first entry of t's list with start >= m.start (lists are sorted by start)
+                    for (;;) {
+                        const uint32_t idx = j + lane;
+                        const bool ge = idx >= tcount || (tl[idx].x & 0xFFFFu) >= m.start;
+                        const uint32_t b = __ballot_sync(kFull, ge);
+                        if (b) {
+                            j += static_cast<uint32_t>(__ffs(b)) - 1u;
+                            break;
+                        }
+                        j += 32u;
+                    }
+                    bool met = false;
+                    if (j < tcount) {
+                        const uint2 e = tl[j];
+                        if (e.x == pack_entry(m).x && e.y == m.off) {
+                            uint32_t e0, e1, e2;
+                            reps_after(tl, j, e0, e1, e2);
+                            met = e0 == s.r0 && e1 == s.r1 && e2 == s.r2;
+                        }
+                    }
+                    if (met) {
+                        if (lane == 0) {
+                            S.sync_warp[warp] = t;
+                            S.sync_idx[warp] = j;
+                        }
                         break;
                     }
-                    j += 32u;
+                    if (cw.n == kContCap) {
+                        if (lane == 0) atomicOr(&S.flags, 1u);  // give up: exact fallback below
+                        break;
+                    }
+                    cw.put(pack_entry(m));
+                }
+                cw.flush();
+                if (lane == 0) S.cont_count[warp] = cw.n;
+            }
+            __syncthreads();
+        } else {
+            // ---- 2a. speculative parse of each segment (one 8-lane group each)
+            const uint32_t sg = tid / GL, gl = lane & (GL - 1u), gb = lane & ~(GL - 1u);
+            const uint32_t seg_start = sg * kSegW, seg_end = seg_start + kSegW;
+            const bool active = seg_start < lim_pos;
+            const bool last_active = !(seg_end < lim_pos);
+            const uint32_t stop = last_active ? size : seg_end;
+            uint2 *lst = seg + sg * kLaneCap;
+            PState s{seg_start, 1u, 4u, 8u};
+            uint32_t n = 0;
+            for (;;) {
+                const bool run = active && s.p < stop && s.p + 3u < size;
+                if (!__any_sync(kFull, run)) break;
+                Match m;
+                if (group_step(win, S.bm, cand, size, lazy, run, s, m)) {
+                    if (gl == 0) lst[n] = pack_entry(m);
+                    ++n;
+                }
+            }
+            if (gl == 0) {
+                S.spec_count[sg] = n;
+                S.cont_count[sg] = 0;
+                S.sync_warp[sg] = kNoWarp;
+                S.sync_idx[sg] = 0;
+            }
+            __syncthreads();
+
+            // ---- 2b. continue each group's parse until it meets a later segment's list
+            bool crun = active && !last_active;
+            uint32_t t = kNoWarp, j = 0, cn = 0;
+            uint2 *cl = lst + kSpecCap;
+            for (;;) {
+                const bool run = crun && s.p + 3u < size;
+                if (!__any_sync(kFull, run)) break;
+                Match m;
+                const bool ev = group_step(win, S.bm, cand, size, lazy, run, s, m);
+                uint32_t tcount = 0;
+                const uint2 *tl = seg;
+                if (ev) {
+                    const uint32_t tw = m.start / kSegW;  // segment that holds this match start
+                    if (tw != t) {
+                        t = tw;
+                        j = 0;
+                    }
+                    tcount = S.spec_count[t];
+                    tl = seg + t * kLaneCap;
+                }
+                // first entry of t's list with start >= m.start (lists are sorted by start), 8 per step
+                bool found = !ev;
+                while (__any_sync(kFull, !found)) {
+                    const uint32_t idx = j + gl;
+                    const bool ge = !found && (idx >= tcount || (tl[idx].x & 0xFFFFu) >= m.start);
+                    const uint32_t b = (__ballot_sync(kFull, ge) >> gb) & ((1u << GL) - 1u);
+                    if (!found) {
+                        if (b) {
+                            j += static_cast<uint32_t>(__ffs(b)) - 1u;
+                            found = true;
+                        } else {
+                            j += GL;
+                        }
+                    }
+                }
+                if (!ev) {
+                    if (!run) crun = false;
+                    continue;
                 }
                 bool met = false;
                 if (j < tcount) {
@@ -540,27 +755,27 @@ __global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBloc
                     }
                 }
                 if (met) {
-                    if (lane == 0) {
-                        S.sync_warp[warp] = t;
-                        S.sync_idx[warp] = j;
+                    if (gl == 0) {
+                        S.sync_warp[sg] = t;
+                        S.sync_idx[sg] = j;
                     }
-                    break;
+                    crun = false;
+                } else if (cn == kContCap) {
+                    if (gl == 0) atomicOr(&S.flags, 1u);  // give up: exact fallback below
+                    crun = false;
+                } else {
+                    if (gl == 0) cl[cn] = pack_entry(m);
+                    ++cn;
                 }
-                if (cw.n == kContCap) {
-                    if (lane == 0) atomicOr(&S.flags, 1u);  // give up: exact fallback below
-                    break;
-                }
-                cw.put(pack_entry(m));
             }
-            cw.flush();
-            if (lane == 0) S.cont_count[warp] = cw.n;
+            if (gl == 0) S.cont_count[sg] = cn;
+            __syncthreads();
         }
-        __syncthreads();
 
         if (!(S.flags & 1u)) {
             // ---- 3. chain walk (one thread), then copy in chain order
             if (tid == 0) {
-                for (uint32_t i = 0; i < kWarps; ++i) S.on_chain[i] = 0;
+                for (uint32_t i = 0; i < kSegs; ++i) S.on_chain[i] = 0;
                 uint32_t cur = 0, from = 0, acc = 0;
                 if (lim_pos > 0) {
                     for (;;) {
@@ -580,12 +795,13 @@ __global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBloc
             const uint32_t total = S.total;
             const uint32_t keep = total < a.max_seqs ? total : a.max_seqs;
             // Write {start, ml-3, off} in order; ll is filled in the next pass.
-            if (S.on_chain[warp]) {
-                const uint32_t from = S.chain_from[warp], ns = S.spec_count[warp], nc = S.cont_count[warp];
-                const uint32_t base = S.out_off[warp];
-                const uint2 *mine = seg + warp * kLaneCap;
+            const uint32_t csg = tid / GL, csl = tid % GL;  // segment whose list this thread copies
+            if (S.on_chain[csg]) {
+                const uint32_t from = S.chain_from[csg], ns = S.spec_count[csg], nc = S.cont_count[csg];
+                const uint32_t base = S.out_off[csg];
+                const uint2 *mine = seg + csg * kLaneCap;
                 uint32_t cov = 0;
-                for (uint32_t i = from + lane; i < ns + nc; i += 32u) {
+                for (uint32_t i = from + csl; i < ns + nc; i += GL) {
                     const uint32_t o = base + (i - from);
                     const uint2 e = mine[i < ns ? i : kSpecCap + (i - ns)];
                     if (o < keep) {
@@ -681,37 +897,41 @@ __global__ void __launch_bounds__(SegCfg<SegW>::kThreads, SegCfg<SegW>::kMinBloc
 
 }  // namespace
 
-// Seg entries per window: the largest of the three layouts, so that a buffer
-// sized once serves every segment width.
+// Seg entries per window: the largest of the layouts, so that a buffer sized
+// once serves every segment width.
+template <uint32_t SegW, uint32_t GL = 32>
+constexpr uint32_t seg_entries() { return SegCfg<SegW, GL>::kSegs * SegCfg<SegW, GL>::kLaneCap; }
 constexpr uint32_t kSegStride = []() constexpr {
-    uint32_t m = SegCfg<2048>::kWarps * SegCfg<2048>::kLaneCap;
-    if (SegCfg<4096>::kWarps * SegCfg<4096>::kLaneCap > m) m = SegCfg<4096>::kWarps * SegCfg<4096>::kLaneCap;
-    if (SegCfg<8192>::kWarps * SegCfg<8192>::kLaneCap > m) m = SegCfg<8192>::kWarps * SegCfg<8192>::kLaneCap;
+    uint32_t m = seg_entries<2048>();
+    if (seg_entries<4096>() > m) m = seg_entries<4096>();
+    if (seg_entries<8192>() > m) m = seg_entries<8192>();
+    if (seg_entries<1024, 8>() > m) m = seg_entries<1024, 8>();
     return m;
 }();
 
 size_t zstd2_seg_scratch_entries(uint32_t num_windows) { return static_cast<size_t>(num_windows) * kSegStride; }
 
 namespace {
-template <bool kRef, uint32_t SegW>
+template <bool kRef, uint32_t SegW, uint32_t GL>
 cudaError_t launch_parse_variant(const Zstd2Args &a, int num_sms, int ctas_per_sm, cudaStream_t st) {
-    using C = SegCfg<SegW>;
-    const uint32_t smem = sizeof(SmemLayout<C::kWarps>);
-    static_assert(sizeof(SmemLayout<C::kWarps>) + 1024 <= 233472 / 3, "three CTAs per SM must fit");
+    using C = SegCfg<SegW, GL>;
+    const uint32_t smem = sizeof(SmemLayout<C::kSegs>);
+    static_assert(sizeof(SmemLayout<C::kSegs>) + 1024 <= 233472 / 3, "three CTAs per SM must fit");
     static SmemOnce smem_set{0};
-    cudaError_t e = set_smem_once(zstd_parse_kernel<kRef, SegW>, smem, smem_set);
+    cudaError_t e = set_smem_once(zstd_parse_kernel<kRef, SegW, GL>, smem, smem_set);
     if (e != cudaSuccess) return e;
     int grid = num_sms * ctas_per_sm;
     if (static_cast<uint32_t>(grid) > a.num_windows) grid = static_cast<int>(a.num_windows);
-    zstd_parse_kernel<kRef, SegW><<<grid, C::kThreads, smem, st>>>(a);
+    zstd_parse_kernel<kRef, SegW, GL><<<grid, C::kThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
 template <bool kRef>
 cudaError_t launch_parse_ref(const Zstd2Args &a, uint32_t seg_width, int num_sms, int ctas_per_sm, cudaStream_t st) {
-    if (seg_width == 2048) return launch_parse_variant<kRef, 2048>(a, num_sms, ctas_per_sm, st);
-    if (seg_width == 8192) return launch_parse_variant<kRef, 8192>(a, num_sms, ctas_per_sm, st);
-    return launch_parse_variant<kRef, 4096>(a, num_sms, ctas_per_sm, st);
+    if (seg_width == 1024) return launch_parse_variant<kRef, 1024, 8>(a, num_sms, ctas_per_sm, st);
+    if (seg_width == 2048) return launch_parse_variant<kRef, 2048, 32>(a, num_sms, ctas_per_sm, st);
+    if (seg_width == 8192) return launch_parse_variant<kRef, 8192, 32>(a, num_sms, ctas_per_sm, st);
+    return launch_parse_variant<kRef, 4096, 32>(a, num_sms, ctas_per_sm, st);
 }
 }  // namespace
 

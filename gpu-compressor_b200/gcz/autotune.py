@@ -5,8 +5,9 @@ decide the sequences and matches); what may change is how the work is
 scheduled:
 
   Zstd   "sweep_warps"  windows swept per CTA (4-7), one 32 KiB table each
-         "parse_seg"    speculative segment per warp in the second stage
-                        (2048, 4096, 8192 bytes: 32, 16 or 8 warps per window)
+         "parse_seg"    speculative segment of the second stage: 2048, 4096 or
+                        8192 bytes per warp (32, 16 or 8 warps per window), or
+                        1024 bytes per 8-lane group (64 segments per window)
          "parse_ctas"   second-stage CTAs per SM
   LZMA2  "lzma_ctas"    second-stage CTAs per SM (the sweep is shared)
   host   "slice_windows" windows per slice of the host-buffer pipelines
@@ -34,7 +35,7 @@ TUNED_DIR = os.path.join(HERE, "tuned")
 ZSTD_CANDIDATES = [
     {"algo": 2, "sweep_warps": sw, "parse_seg": seg, "parse_ctas": ctas}
     for sw in (7, 6, 5, 4)
-    for seg, ctas_list in ((4096, (3, 2)), (8192, (3, 2)), (2048, (1,)))
+    for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (8192, (3, 2)), (2048, (1,)))
     for ctas in ctas_list
 ]
 LZMA_CANDIDATES = [{"lzma_ctas": c} for c in (3, 2, 1)]

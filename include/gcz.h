@@ -74,8 +74,12 @@ const char *gcz_version(void);
 /* Schedule-only knobs (they never change results): "algo" = 2 (default) runs
  * the candidate sweep then the per-window second stage, 1 the fused
  * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
- * memory with bulk copies, 0 reads it through L1; "parse_ctas" = second-stage
- * CTAs per SM (1-8); "slice_windows" = windows per slice of the host-buffer
+ * memory with bulk copies, 0 reads it through L1; "parse_ctas" = Zstd
+ * second-stage CTAs per SM (1-8); "parse_seg" = the Zstd second stage's
+ * speculative segment: 2048, 4096 (default) or 8192 bytes per warp, or 1024
+ * bytes per 8-lane group; "sweep_warps" = windows per candidate-sweep CTA
+ * (4-7, default 7); "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
+ * default 3); "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 1024 = 64 MiB; four slots, three slices in flight;
  * slices ramp up from a quarter of it and back down at the end);
  * "frames_slice_windows" =

@@ -39,9 +39,11 @@ def run_ref_layout(ctx, data, window, depth, max_seqs):
             sc.cpu().numpy().view(np.uint32)[:B], lc.cpu().numpy().view(np.uint32)[:B])
 
 
-@pytest.mark.parametrize("algo,staged", [(2, 1), (1, 1), (1, 0)], ids=["split", "fused-staged", "fused-l1"])
+@pytest.mark.parametrize("algo,staged,seg", [(2, 1, 4096), (2, 1, 1024), (2, 1, 2048), (2, 1, 8192), (1, 1, 4096),
+                                             (1, 0, 4096)],
+                         ids=["split", "split-group1k", "split-seg2k", "split-seg8k", "fused-staged", "fused-l1"])
 @pytest.mark.parametrize("name,spec", cases.CASES, ids=[n for n, _ in cases.CASES])
-def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged):
+def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged, seg):
     z, meta = golden
     m = next(x for x in meta if x["name"] == name)
     data = cases.build(spec)
@@ -49,11 +51,13 @@ def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, stag
     W = spec["window"]
     ctx.set_option("algo", algo)
     ctx.set_option("staged", staged)
+    ctx.set_option("parse_seg", seg)
     try:
         seqs, lits, sc, lc = run_ref_layout(ctx, data, W, spec["zdepth"], spec["max_seqs"])
     finally:
         ctx.set_option("algo", 2)
         ctx.set_option("staged", 1)
+        ctx.set_option("parse_seg", 4096)
     np.testing.assert_array_equal(sc, z[f"{name}/zstd_seq_counts"])
     np.testing.assert_array_equal(lc, z[f"{name}/zstd_lit_counts"])
     flat = np.concatenate([seqs[b, :sc[b]] for b in range(sc.size)]) if sc.size else np.zeros((0, 3), np.uint32)
@@ -72,20 +76,22 @@ def test_compact_host_api_matches_oracle(ctx, name, spec):
     np.testing.assert_array_equal(seqs, o_seqs)
 
 
-@pytest.mark.parametrize("algo", [2, 1])
+@pytest.mark.parametrize("algo,seg", [(2, 4096), (2, 1024), (1, 4096)], ids=["split", "split-group1k", "fused"])
 @pytest.mark.parametrize("seed,n,mix", [(1, 16 << 20, (0.4, 0.4, 0.2)), (31, 5 << 20, (0.05, 0.9, 0.05)),
                                         (32, 3 << 20 | 12345, (0.9, 0.05, 0.05)), (33, 2 << 20, (0.0, 0.0, 1.0)),
                                         (34, 2 << 20, (0.0, 1.0, 0.0))])
-def test_synthetic_vs_oracle(ctx, seed, n, mix, algo):
+def test_synthetic_vs_oracle(ctx, seed, n, mix, algo, seg):
     """Zstd L1 plain workload shape (16 MiB, seed 1) and skewed mixes."""
     import gcz
 
     data = gcz.gen_synthetic(seed, n, 8 << 20, mix)
     ctx.set_option("algo", algo)
+    ctx.set_option("parse_seg", seg)
     try:
         seqs, offsets = ctx.zstd_match_find(data, 16)
     finally:
         ctx.set_option("algo", 2)
+        ctx.set_option("parse_seg", 4096)
     o_seqs, o_off = orc.zstd_sequences(data, 16, threads=16)
     np.testing.assert_array_equal(offsets, o_off)
     np.testing.assert_array_equal(seqs, o_seqs)
