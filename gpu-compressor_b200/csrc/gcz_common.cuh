@@ -116,14 +116,6 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
-// Hint: pull [src, src + bytes) into L2 (bulk prefetch, no completion to wait
-// for).  src 16-byte aligned; bytes are rounded down to a multiple of 16.
-__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
-    bytes &= ~15u;
-    if (bytes)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
-
 // Bounded wait on an mbarrier phase: true when the phase completed, false when
 // the iteration limit ran out (each try_wait already suspends for a while).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_iter = (1u << 24)) {

@@ -242,14 +242,6 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
         const uint64_t start = a.wins ? a.wins[wi].offset : static_cast<uint64_t>(wi) * a.window;
         const uint32_t size =
             a.wins ? a.wins[wi].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
-        if (tid == 0 && wi + gridDim.x < a.num_windows) {  // this CTA's next window and candidates into L2
-            const uint32_t nw = wi + gridDim.x;
-            const uint64_t ns = a.wins ? a.wins[nw].offset : static_cast<uint64_t>(nw) * a.window;
-            const uint32_t nsz =
-                a.wins ? a.wins[nw].size : static_cast<uint32_t>(a.n - ns < a.window ? a.n - ns : a.window);
-            prefetch_l2(a.src + ns, nsz);
-            prefetch_l2(a.cand + ns, 2u * nsz);
-        }
         __syncthreads();
         if (tid == 0) {
             S.any = 0;

@@ -49,12 +49,6 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
         const uint64_t start = a.wins ? a.wins[w].offset : static_cast<uint64_t>(w) * a.window;
         const uint32_t size =
             a.wins ? a.wins[w].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
-        if (lane == 0 && w + gwarps < a.num_windows) {  // this warp's next window into L2
-            const uint32_t nw = w + gwarps;
-            const uint64_t ns = a.wins ? a.wins[nw].offset : static_cast<uint64_t>(nw) * a.window;
-            prefetch_l2(a.src + ns,
-                        a.wins ? a.wins[nw].size : static_cast<uint32_t>(a.n - ns < a.window ? a.n - ns : a.window));
-        }
         for (uint32_t i = lane; i < kHashSize * 2 / 16; i += 32) T4[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
         __syncwarp();
         const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);

@@ -558,14 +558,6 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             a.wins ? a.wins[wi].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
         const uint16_t *cand = a.cand + start;
         uint2 *seg = a.seg + static_cast<uint64_t>(wi) * a.seg_stride;
-        if (tid == 0 && wi + gridDim.x < a.num_windows) {  // this CTA's next window and candidates into L2
-            const uint32_t nw = wi + gridDim.x;
-            const uint64_t ns = a.wins ? a.wins[nw].offset : static_cast<uint64_t>(nw) * a.window;
-            const uint32_t nsz =
-                a.wins ? a.wins[nw].size : static_cast<uint32_t>(a.n - ns < a.window ? a.n - ns : a.window);
-            prefetch_l2(a.src + ns, nsz);
-            prefetch_l2(a.cand + ns, 2u * nsz);
-        }
 
         // ---- 1. stage the window (warp 0), verification bitmap (all warps)
         __syncthreads();  // previous window fully consumed
