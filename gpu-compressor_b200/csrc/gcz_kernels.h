@@ -71,9 +71,12 @@ struct Zstd2Launch {
 };
 
 cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
-// sweep_warps: windows swept per CTA (4-7, one 32 KiB table each; schedule only).
+// sweep_warps: windows swept per CTA (4-7, one 32 KiB table each); sweep_groups:
+// lanes with equal hashes in a step grouped by __match_any_sync (0) or by
+// bit-sliced ballots (1).  Both are schedule only.
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st, const WinDesc *wins = nullptr, int sweep_warps = 7);
+                              int num_sms, cudaStream_t st, const WinDesc *wins = nullptr, int sweep_warps = 7,
+                              int sweep_groups = 0);
 size_t zstd2_seg_scratch_entries(uint32_t num_windows);
 cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st);
 cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);

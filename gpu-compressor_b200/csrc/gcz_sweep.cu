@@ -35,9 +35,27 @@ struct SweepArgs {
     const WinDesc *wins;
 };
 
+// Lanes of this warp whose key equals this lane's (valid lanes only; an
+// invalid lane matches only itself): kBits ballots, one per key bit, combined
+// bit-sliced.  The ballots do not depend on each other, so their latency
+// overlaps, unlike one __match_any_sync.
+template <int kBits>
+__device__ __forceinline__ uint32_t same_key_lanes(uint32_t key, bool valid) {
+    uint32_t m = __ballot_sync(kFull, valid);
+#pragma unroll
+    for (int b = 0; b < kBits; ++b) {
+        const bool bit = (key >> b) & 1u;
+        const uint32_t bb = __ballot_sync(kFull, bit);
+        m &= bit ? bb : ~bb;
+    }
+    return valid ? m : (1u << lane_id());
+}
+
 // kSweepWarpsPerCta windows per CTA, one 32 KiB table each (7 fill an SM's
-// shared memory); a schedule knob, the candidates do not depend on it.
-template <int kSweepWarpsPerCta>
+// shared memory); a schedule knob, the candidates do not depend on it.  So is
+// kBallotGroups: how the lanes of a step with equal hashes are grouped
+// (__match_any_sync, or bit-sliced ballots).
+template <int kSweepWarpsPerCta, bool kBallotGroups>
 __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -112,7 +130,10 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
                 for (uint32_t j = 0; j < 4; ++j) {
                     if (j < j0) continue;
                     const uint32_t q = blk * 128u + j * 32u + lane;
-                    if ((dsteps >> j) & 1u) g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+                    if ((dsteps >> j) & 1u) {
+                        if constexpr (kBallotGroups) g[j] = same_key_lanes<kHashLog>(h[j], v[j]);
+                        else g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+                    }
                     tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
                     __syncwarp();
                     if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
@@ -137,31 +158,32 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
 }  // namespace
 
 namespace {
-template <int kWarps>
+template <int kWarps, bool kBallotGroups>
 cudaError_t launch_sweep_variant(const SweepArgs &a, int num_sms, cudaStream_t st) {
     const uint32_t smem = kWarps * kHashSize * sizeof(uint16_t);
     static SmemOnce smem_set{0};
-    cudaError_t e = set_smem_once(cand_sweep_kernel<kWarps>, smem, smem_set);
+    cudaError_t e = set_smem_once(cand_sweep_kernel<kWarps, kBallotGroups>, smem, smem_set);
     if (e != cudaSuccess) return e;
     // as many CTAs per SM as the tables allow (one for 5-7 warps, two for 4 or less)
     const uint32_t per_sm = (227u * 1024u) / (smem + 1024u);
     uint32_t ctas = (a.num_windows + kWarps - 1) / kWarps;
     const uint32_t cap = static_cast<uint32_t>(num_sms) * (per_sm ? per_sm : 1u);
     if (ctas > cap) ctas = cap;
-    cand_sweep_kernel<kWarps><<<ctas, 32 * kWarps, smem, st>>>(a);
+    cand_sweep_kernel<kWarps, kBallotGroups><<<ctas, 32 * kWarps, smem, st>>>(a);
     return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps) {
+                              int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps, int sweep_groups) {
     if (num_windows == 0) return cudaSuccess;
     SweepArgs a{src, n, window, num_windows, cand, wins};
+    const bool ballots = sweep_groups != 0;
     switch (sweep_warps) {
-    case 4: return launch_sweep_variant<4>(a, num_sms, st);
-    case 5: return launch_sweep_variant<5>(a, num_sms, st);
-    case 6: return launch_sweep_variant<6>(a, num_sms, st);
-    default: return launch_sweep_variant<7>(a, num_sms, st);
+    case 4: return ballots ? launch_sweep_variant<4, true>(a, num_sms, st) : launch_sweep_variant<4, false>(a, num_sms, st);
+    case 5: return ballots ? launch_sweep_variant<5, true>(a, num_sms, st) : launch_sweep_variant<5, false>(a, num_sms, st);
+    case 6: return ballots ? launch_sweep_variant<6, true>(a, num_sms, st) : launch_sweep_variant<6, false>(a, num_sms, st);
+    default: return ballots ? launch_sweep_variant<7, true>(a, num_sms, st) : launch_sweep_variant<7, false>(a, num_sms, st);
     }
 }
 

@@ -116,6 +116,15 @@ struct Win {
         const uint32_t a = static_cast<uint32_t>(q + static_cast<int>(kPre));
         return __funnelshift_r(w[a >> 2], w[(a >> 2) + 1], (a & 3u) * 8u);
     }
+    // The 8 bytes at q: three aligned words, two funnel shifts.
+    __device__ __forceinline__ void u64(int q, uint32_t &lo, uint32_t &hi) const {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(d - kPre);
+        const uint32_t a = static_cast<uint32_t>(q + static_cast<int>(kPre));
+        const uint32_t i = a >> 2, sh = (a & 3u) * 8u;
+        const uint32_t w1 = w[i + 1];
+        lo = __funnelshift_r(w[i], w1, sh);
+        hi = __funnelshift_r(w1, w[i + 2], sh);
+    }
 };
 
 // First index in [0, lim) where bytes c+i and q+i differ, else lim.
@@ -398,21 +407,25 @@ __device__ __forceinline__ uint32_t extend_group(const Win &w, uint32_t c, uint3
     uint32_t len = 0, out = 0;
     bool done = !act;
     while (__any_sync(kFull, !done)) {
-        const uint32_t k = len + 4u * gl;
+        const uint32_t k = len + 8u * gl;  // 8 bytes per lane
         uint32_t res = k;
         if (!done && k < lim) {
-            const uint32_t d = w.u32(static_cast<int>(q + k)) ^ w.u32(static_cast<int>(c + k));
-            const uint32_t fb = d ? (static_cast<uint32_t>(__ffs(d)) - 1u) >> 3 : 4u;
+            uint32_t ql, qh, cl, ch;
+            w.u64(static_cast<int>(q + k), ql, qh);
+            w.u64(static_cast<int>(c + k), cl, ch);
+            const uint32_t dl = ql ^ cl, dh = qh ^ ch;
+            const uint32_t fb = dl ? (static_cast<uint32_t>(__ffs(dl)) - 1u) >> 3
+                                   : (dh ? 4u + ((static_cast<uint32_t>(__ffs(dh)) - 1u) >> 3) : 8u);
             const uint32_t rem = lim - k;
             res = k + (fb < rem ? fb : rem);
         }
-        const uint32_t sb = (__ballot_sync(kFull, !done && res < k + 4u) >> gb) & ((1u << GL) - 1u);
+        const uint32_t sb = (__ballot_sync(kFull, !done && res < k + 8u) >> gb) & ((1u << GL) - 1u);
         const uint32_t v = __shfl_sync(kFull, res, gb + (sb ? static_cast<uint32_t>(__ffs(sb)) - 1u : 0u));
         if (!done && sb) {
             out = v;
             done = true;
         }
-        len += 4u * GL;
+        len += 8u * GL;
     }
     return out;
 }
@@ -439,16 +452,20 @@ __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, con
     const uint32_t j0 = 4u * gl;
     const uint32_t q0 = j0 < nh ? p + j0 : p;
     const uint32_t vlim = j0 < nh ? (nh - j0 < 4u ? nh - j0 : 4u) : 0u;  // positions of this lane to test
-    const uint32_t xlo = w.u32(static_cast<int>(q0)), xhi = w.u32(static_cast<int>(q0 + 4u));
+    const uint32_t vall = (1u << vlim) - 1u;
+    uint32_t xlo, xhi;
+    w.u64(static_cast<int>(q0), xlo, xhi);
     uint32_t mk[3];
 #pragma unroll
     for (uint32_t k = 0; k < 3; ++k) {
         const uint32_t rv = k == 0u ? s.r0 : (k == 1u ? s.r1 : s.r2);
         // positions q0 + t with t < vlim and q0 + t >= rv; their source bytes start at q0 - rv + t >= 0
-        const uint32_t tmin = rv > q0 ? rv - q0 : 0u;
-        const uint32_t valid = tmin < vlim ? ((1u << vlim) - 1u) & ~((1u << tmin) - 1u) : 0u;
+        // (rv > q0 only within 3 bytes of a window or segment start)
+        const uint32_t valid = rv <= q0 ? vall : (rv - q0 < vlim ? vall & (~0u << (rv - q0)) : 0u);
         const int yb = valid ? static_cast<int>(q0) - static_cast<int>(rv) : static_cast<int>(q0);
-        const uint32_t dlo = xlo ^ w.u32(yb), dhi = xhi ^ w.u32(yb + 4);
+        uint32_t ylo, yhi;
+        w.u64(yb, ylo, yhi);
+        const uint32_t dlo = xlo ^ ylo, dhi = xhi ^ yhi;
         const uint32_t e = ((dlo & 0xFFFFFFu) == 0u ? 1u : 0u) | ((dlo >> 8) == 0u ? 2u : 0u) |
                            ((__funnelshift_r(dlo, dhi, 16) & 0xFFFFFFu) == 0u ? 4u : 0u) |
                            ((__funnelshift_r(dlo, dhi, 24) & 0xFFFFFFu) == 0u ? 8u : 0u);

@@ -78,7 +78,9 @@ const char *gcz_version(void);
  * second-stage CTAs per SM (1-8); "parse_seg" = the Zstd second stage's
  * speculative segment: 2048, 4096 (default) or 8192 bytes per warp, or 1024
  * bytes per 8-lane group; "sweep_warps" = windows per candidate-sweep CTA
- * (4-7, default 7); "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
+ * (4-7, default 7); "sweep_groups" = how the sweep groups the lanes of a step
+ * that share a hash bucket (0: __match_any_sync, 1: bit-sliced ballots);
+ * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
  * default 3); "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 1024 = 64 MiB; four slots, three slices in flight;
  * slices ramp up from a quarter of it and back down at the end);
