@@ -67,12 +67,12 @@ struct gcz_ctx {
     uint32_t *d_status = nullptr;
     Scratch sc;      // scratch of the _device entry points
     Slot slots[4];   // host-buffer pipelines: each rotates over all four, three slices in flight
-    uint32_t slice_windows = 1024;         // windows per pipeline slice (64 MiB)
+    uint32_t slice_windows = 512;          // windows per pipeline slice (32 MiB)
     uint32_t frames_slice_windows = 512;   // ... of the GPU frames pipeline (32 MiB, four slots)
     int staged = 1;
     int algo = 2;          // 1: fused single-warp kernels, 2: candidate sweep + second stage
     int parse_ctas = 3;    // second-stage CTAs per SM
-    int seg_width = 4096;  // Zstd speculative segment bytes per warp (2048, 4096, 8192)
+    int seg_width = 1024;  // Zstd speculative segment: 1024 per 8-lane group, or 2048/4096/8192 per warp
     int sweep_warps = 7;   // candidate-sweep windows per CTA (4-7)
     int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0 __match_any_sync, 1 bit-sliced ballots
     int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM

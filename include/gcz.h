@@ -76,13 +76,13 @@ const char *gcz_version(void);
  * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
  * memory with bulk copies, 0 reads it through L1; "parse_ctas" = Zstd
  * second-stage CTAs per SM (1-8); "parse_seg" = the Zstd second stage's
- * speculative segment: 2048, 4096 (default) or 8192 bytes per warp, or 1024
- * bytes per 8-lane group; "sweep_warps" = windows per candidate-sweep CTA
+ * speculative segment: 1024 bytes per 8-lane group (default), or 2048, 4096
+ * or 8192 bytes per warp; "sweep_warps" = windows per candidate-sweep CTA
  * (4-7, default 7); "sweep_groups" = how the sweep groups the lanes of a step
  * that share a hash bucket (0: __match_any_sync, 1: bit-sliced ballots);
  * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
  * default 3); "slice_windows" = windows per slice of the host-buffer
- * pipelines (default 1024 = 64 MiB; four slots, three slices in flight;
+ * pipelines (default 512 = 32 MiB; four slots, three slices in flight;
  * slices ramp up from a quarter of it and back down at the end);
  * "frames_slice_windows" =
  * the same for gcz_zstd_compress_frames_gpu (default 512 = 32 MiB; four

@@ -57,7 +57,7 @@ def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, stag
     finally:
         ctx.set_option("algo", 2)
         ctx.set_option("staged", 1)
-        ctx.set_option("parse_seg", 4096)
+        ctx.set_option("parse_seg", 1024)
     np.testing.assert_array_equal(sc, z[f"{name}/zstd_seq_counts"])
     np.testing.assert_array_equal(lc, z[f"{name}/zstd_lit_counts"])
     flat = np.concatenate([seqs[b, :sc[b]] for b in range(sc.size)]) if sc.size else np.zeros((0, 3), np.uint32)
@@ -91,7 +91,7 @@ def test_synthetic_vs_oracle(ctx, seed, n, mix, algo, seg):
         seqs, offsets = ctx.zstd_match_find(data, 16)
     finally:
         ctx.set_option("algo", 2)
-        ctx.set_option("parse_seg", 4096)
+        ctx.set_option("parse_seg", 1024)
     o_seqs, o_off = orc.zstd_sequences(data, 16, threads=16)
     np.testing.assert_array_equal(offsets, o_off)
     np.testing.assert_array_equal(seqs, o_seqs)
