@@ -74,7 +74,7 @@ struct gcz_ctx {
     int parse_ctas = 3;    // second-stage CTAs per SM
     int seg_width = 1024;  // Zstd speculative segment: 1024 per 8-lane group, or 2048/4096/8192 per warp
     int sweep_warps = 7;   // candidate-sweep windows per CTA (4-7)
-    int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0 __match_any_sync, 1 bit-sliced ballots
+    int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0/1 after a read-back (match_any/ballots), 2/3 one block ahead
     int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM
     // profiling
     bool prof = false;
@@ -452,7 +452,7 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->sweep_warps = (int)value;
         return GCZ_OK;
     }
-    if (!strcmp(key, "sweep_groups") && (value == 0 || value == 1)) {
+    if (!strcmp(key, "sweep_groups") && value >= 0 && value <= 3) {
         c->sweep_groups = (int)value;
         return GCZ_OK;
     }

@@ -72,8 +72,9 @@ struct Zstd2Launch {
 
 cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
 // sweep_warps: windows swept per CTA (4-7, one 32 KiB table each); sweep_groups:
-// lanes with equal hashes in a step grouped by __match_any_sync (0) or by
-// bit-sliced ballots (1).  Both are schedule only.
+// lanes with equal hashes in a step grouped by __match_any_sync (0, 2) or by
+// bit-sliced ballots (1, 3), after a table read-back in the blocks that have
+// such lanes (0, 1) or for every step one block ahead (2, 3).  Schedule only.
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
                               int num_sms, cudaStream_t st, const WinDesc *wins = nullptr, int sweep_warps = 7,
                               int sweep_groups = 0);

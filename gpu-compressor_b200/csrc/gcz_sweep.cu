@@ -155,21 +155,107 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
     }
 }
 
+// The same candidates with each step's lanes grouped by hash one block
+// ahead.  Which lanes of a step share a bucket depends only on the input
+// bytes, so the groups of block b+1 are formed (by __match_any_sync or by
+// bit-sliced ballots) while block b's table work runs, and their latency
+// overlaps it.  With the groups known, each step is one read (every lane reads
+// its bucket: the lowest lane of a group gets the table's candidate, the others
+// take the next lower lane's position) and one write (the highest lane of each
+// group), with no read-back and no redo.
+template <bool kBallots>
+__device__ __forceinline__ void block_hashes(uint32_t blk, uint32_t size, uint32_t w0, uint32_t w1, uint32_t *h,
+                                             bool *v, uint32_t *g) {
+    const uint32_t lane = lane_id();
+    const uint32_t up = __shfl_down_sync(kFull, w0, 1);
+    const uint32_t n0 = __shfl_sync(kFull, w1, 0);
+    const uint32_t w0n = lane == 31u ? n0 : up;  // word l+1
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t q = blk * 128u + j * 32u + lane;
+        const uint32_t src_lane = j * 8u + (lane >> 2);
+        const uint32_t lo = __shfl_sync(kFull, w0, src_lane);
+        const uint32_t hi = __shfl_sync(kFull, w0n, src_lane);
+        v[j] = q + 3u < size;
+        h[j] = hash4(__funnelshift_r(lo, hi, (lane & 3u) * 8u));
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        if constexpr (kBallots) g[j] = same_key_lanes<kHashLog>(h[j], v[j]);
+        else g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+    }
+}
+
+template <int kSweepWarpsPerCta, bool kBallots>
+__global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_ahead_kernel(SweepArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    uint16_t *T = reinterpret_cast<uint16_t *>(smem) + warp * kHashSize;
+    uint4 *T4 = reinterpret_cast<uint4 *>(T);
+    const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
+    const uint32_t gwarps = gridDim.x * kSweepWarpsPerCta;
+    for (uint32_t w = blockIdx.x * kSweepWarpsPerCta + warp; w < a.num_windows; w += gwarps) {
+        const uint64_t start = a.wins ? a.wins[w].offset : static_cast<uint64_t>(w) * a.window;
+        const uint32_t size =
+            a.wins ? a.wins[w].size : static_cast<uint32_t>(a.n - start < a.window ? a.n - start : a.window);
+        for (uint32_t i = lane; i < kHashSize * 2 / 16; i += 32) T4[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        __syncwarp();
+        const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);
+        const uint32_t nwords = (size + 3u) >> 2;
+        uint16_t *out = a.cand + start;
+        uint32_t w0 = lane < nwords ? __ldg(src32 + lane) : 0u;
+        uint32_t w1 = 32u + lane < nwords ? __ldg(src32 + 32u + lane) : 0u;
+        uint32_t h[4], g[4];
+        bool v[4];
+        block_hashes<kBallots>(0u, size, w0, w1, h, v, g);
+        for (uint32_t blk = 0; blk * 128u < size; ++blk) {
+            const uint32_t nw = (blk + 2u) * 32u + lane;
+            const uint32_t w2 = nw < nwords ? __ldg(src32 + nw) : 0u;
+            // the next block's hashes and groups: no dependence on the table
+            uint32_t hn[4], gn[4];
+            bool vn[4];
+            block_hashes<kBallots>(blk + 1u, size, w1, w2, hn, vn, gn);
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                const uint32_t q = blk * 128u + j * 32u + lane;
+                const uint32_t tv = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
+                __syncwarp();
+                if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
+                __syncwarp();
+                const uint32_t lower = g[j] & lt;
+                const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv;
+                if (q < size) out[q] = static_cast<uint16_t>(c);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < 4; ++j) {
+                h[j] = hn[j];
+                v[j] = vn[j];
+                g[j] = gn[j];
+            }
+            w0 = w1;
+            w1 = w2;
+        }
+        __syncwarp();
+    }
+}
+
 }  // namespace
 
 namespace {
-template <int kWarps, bool kBallotGroups>
+template <int kWarps, int kMode>
 cudaError_t launch_sweep_variant(const SweepArgs &a, int num_sms, cudaStream_t st) {
+    constexpr bool kBallots = (kMode & 1) != 0, kAhead = kMode >= 2;
+    const auto kernel = kAhead ? cand_sweep_ahead_kernel<kWarps, kBallots> : cand_sweep_kernel<kWarps, kBallots>;
     const uint32_t smem = kWarps * kHashSize * sizeof(uint16_t);
     static SmemOnce smem_set{0};
-    cudaError_t e = set_smem_once(cand_sweep_kernel<kWarps, kBallotGroups>, smem, smem_set);
+    cudaError_t e = set_smem_once(kernel, smem, smem_set);
     if (e != cudaSuccess) return e;
     // as many CTAs per SM as the tables allow (one for 5-7 warps, two for 4 or less)
     const uint32_t per_sm = (227u * 1024u) / (smem + 1024u);
     uint32_t ctas = (a.num_windows + kWarps - 1) / kWarps;
     const uint32_t cap = static_cast<uint32_t>(num_sms) * (per_sm ? per_sm : 1u);
     if (ctas > cap) ctas = cap;
-    cand_sweep_kernel<kWarps, kBallotGroups><<<ctas, 32 * kWarps, smem, st>>>(a);
+    kernel<<<ctas, 32 * kWarps, smem, st>>>(a);
     return cudaGetLastError();
 }
 }  // namespace
@@ -178,12 +264,17 @@ cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, u
                               int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps, int sweep_groups) {
     if (num_windows == 0) return cudaSuccess;
     SweepArgs a{src, n, window, num_windows, cand, wins};
-    const bool ballots = sweep_groups != 0;
-    switch (sweep_warps) {
-    case 4: return ballots ? launch_sweep_variant<4, true>(a, num_sms, st) : launch_sweep_variant<4, false>(a, num_sms, st);
-    case 5: return ballots ? launch_sweep_variant<5, true>(a, num_sms, st) : launch_sweep_variant<5, false>(a, num_sms, st);
-    case 6: return ballots ? launch_sweep_variant<6, true>(a, num_sms, st) : launch_sweep_variant<6, false>(a, num_sms, st);
-    default: return ballots ? launch_sweep_variant<7, true>(a, num_sms, st) : launch_sweep_variant<7, false>(a, num_sms, st);
+    // sweep_groups: 0 / 1 group equal-hash lanes (__match_any_sync / ballots)
+    // only in blocks that need it, after a read-back; 2 / 3 form every step's
+    // groups one block ahead.
+    switch (sweep_groups * 8 + sweep_warps) {
+#define GCZ_SWEEP_CASE(M, W) \
+    case M * 8 + W: return launch_sweep_variant<W, M>(a, num_sms, st);
+#define GCZ_SWEEP_MODE(M) GCZ_SWEEP_CASE(M, 4) GCZ_SWEEP_CASE(M, 5) GCZ_SWEEP_CASE(M, 6) GCZ_SWEEP_CASE(M, 7)
+        GCZ_SWEEP_MODE(0) GCZ_SWEEP_MODE(1) GCZ_SWEEP_MODE(2) GCZ_SWEEP_MODE(3)
+#undef GCZ_SWEEP_MODE
+#undef GCZ_SWEEP_CASE
+    default: return launch_sweep_variant<7, 0>(a, num_sms, st);
     }
 }
 

@@ -5,8 +5,9 @@ decide the sequences and matches); what may change is how the work is
 scheduled:
 
   Zstd   "sweep_warps"  windows swept per CTA (4-7), one 32 KiB table each
-         "sweep_groups" the sweep's grouping of lanes that share a hash bucket
-                        (0: __match_any_sync, 1: bit-sliced ballots)
+         "sweep_groups" the sweep's grouping of lanes that share a hash bucket:
+                        after a read-back (0: __match_any_sync, 1: ballots) or
+                        one block ahead for every step (2, 3 likewise)
          "parse_seg"    speculative segment of the second stage: 2048, 4096 or
                         8192 bytes per warp (32, 16 or 8 warps per window), or
                         1024 bytes per 8-lane group (64 segments per window)
@@ -37,7 +38,7 @@ TUNED_DIR = os.path.join(HERE, "tuned")
 ZSTD_CANDIDATES = [
     {"algo": 2, "sweep_warps": sw, "sweep_groups": sg, "parse_seg": seg, "parse_ctas": ctas}
     for sw in (7, 6, 5, 4)
-    for sg in (0, 1)
+    for sg in (0, 1, 2, 3)
     for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (8192, (3, 2)), (2048, (1,)))
     for ctas in ctas_list
 ]

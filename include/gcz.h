@@ -79,7 +79,9 @@ const char *gcz_version(void);
  * speculative segment: 1024 bytes per 8-lane group (default), or 2048, 4096
  * or 8192 bytes per warp; "sweep_warps" = windows per candidate-sweep CTA
  * (4-7, default 7); "sweep_groups" = how the sweep groups the lanes of a step
- * that share a hash bucket (0: __match_any_sync, 1: bit-sliced ballots);
+ * that share a hash bucket: after a table read-back, only in blocks that have
+ * such lanes, with __match_any_sync (0, default) or bit-sliced ballots (1), or
+ * for every step one block ahead of the table work (2, 3 likewise);
  * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
  * default 3); "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 512 = 32 MiB; four slots, three slices in flight;
