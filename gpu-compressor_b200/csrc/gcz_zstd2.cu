@@ -30,8 +30,9 @@
 //    that hold no hash match -- a ballot finds the first event, matches are
 //    extended 128 bytes per warp iteration, and one lazy step (:278-307)
 //    follows.
-// 3. The chain is written as packed {ll | (ml-3) << 16, off} (or the
-//    reference's {ll, ml-3, off} triples) at the per-window stride, capped at
+// 3. The chain is written in one pass as packed {ll | (ml-3) << 16, off} (or
+//    the reference's {ll, ml-3, off} triples) at the per-window stride, each
+//    literal length taken from the entry before it, capped at
 //    max_seqs exactly like the reference's `num_seqs < max_sequences_per_chunk`
 //    test (:309): the capped parse emits the first max_seqs matches of the
 //    uncapped one and nothing after them.
@@ -75,7 +76,7 @@ constexpr uint32_t kBmWords = kMaxWindow / 32 + 8;  // the wide scan reads up to
 template <uint32_t kSegs>
 struct SmemLayout {
     uint8_t data[kDataBytes];
-    uint32_t bm[kBmWords];  // after the parse, its first kThreads words hold match ends (phase 3)
+    uint32_t bm[kBmWords];
     uint32_t spec_count[kSegs];
     uint32_t cont_count[kSegs];
     uint32_t sync_warp[kSegs];
@@ -83,7 +84,7 @@ struct SmemLayout {
     uint32_t chain_from[kSegs];
     uint32_t out_off[kSegs];
     uint32_t on_chain[kSegs];
-    uint32_t carry;
+    uint32_t prev_end[kSegs];  // end of the match before a chain segment's first copied entry
     uint32_t flags;
     uint32_t total;
     uint32_t covered;
@@ -555,7 +556,6 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
     using C = SegCfg<SegW, GL>;
     constexpr uint32_t kSegW = C::kSegW, kWarps = C::kWarps, kThreads = C::kThreads, kSegs = C::kSegs;
     constexpr uint32_t kSpecCap = C::kSpecCap, kLaneCap = C::kLaneCap, kContCap = C::kContCap;
-    static_assert(kBmWords >= kThreads, "phase 3 reuses the bitmap for match ends");
     extern __shared__ __align__(128) uint8_t smem_raw[];
     SmemLayout<kSegs> &S = *reinterpret_cast<SmemLayout<kSegs> *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -785,13 +785,19 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             // ---- 3. chain walk (one thread), then copy in chain order
             if (tid == 0) {
                 for (uint32_t i = 0; i < kSegs; ++i) S.on_chain[i] = 0;
-                uint32_t cur = 0, from = 0, acc = 0;
+                uint32_t cur = 0, from = 0, acc = 0, pend = 0;
                 if (lim_pos > 0) {
                     for (;;) {
                         S.on_chain[cur] = 1;
                         S.chain_from[cur] = from;
                         S.out_off[cur] = acc;
-                        acc += (S.spec_count[cur] - from) + S.cont_count[cur];
+                        S.prev_end[cur] = pend;
+                        const uint32_t ns = S.spec_count[cur], nc = S.cont_count[cur];
+                        acc += (ns - from) + nc;
+                        if (ns + nc > from) {  // the last entry this segment contributes
+                            const uint2 e = seg[cur * kLaneCap + (nc ? kSpecCap + nc - 1u : ns - 1u)];
+                            pend = (e.x & 0xFFFFu) + (e.x >> 16) + kMinMatch;
+                        }
                         const uint32_t nx = S.sync_warp[cur];
                         if (nx == kNoWarp) break;
                         from = S.sync_idx[cur];
@@ -803,7 +809,10 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             __syncthreads();
             const uint32_t total = S.total;
             const uint32_t keep = total < a.max_seqs ? total : a.max_seqs;
-            // Write {start, ml-3, off} in order; ll is filled in the next pass.
+            // Write {ll, ml-3, off} in chain order: an entry's literal length is
+            // its start minus the end of the entry before it -- the previous
+            // entry of the same list, or for a segment's first copied entry the
+            // last entry of the previous chain segment (from the chain walk).
             const uint32_t csg = tid / GL, csl = tid % GL;  // segment whose list this thread copies
             if (S.on_chain[csg]) {
                 const uint32_t from = S.chain_from[csg], ns = S.spec_count[csg], nc = S.cont_count[csg];
@@ -812,60 +821,28 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
                 uint32_t cov = 0;
                 for (uint32_t i = from + csl; i < ns + nc; i += GL) {
                     const uint32_t o = base + (i - from);
+                    if (o >= keep) break;
                     const uint2 e = mine[i < ns ? i : kSpecCap + (i - ns)];
-                    if (o < keep) {
-                        cov += (e.x >> 16) + kMinMatch;
-                        if constexpr (kRef) {
-                            uint32_t *r = a.ref_seqs + (static_cast<uint64_t>(wi) * a.max_seqs + o) * 3u;
-                            r[0] = e.x & 0xFFFFu;  // start for now
-                            r[1] = e.x >> 16;
-                            r[2] = e.y;
-                        } else {
-                            a.packed[static_cast<uint64_t>(wi) * a.max_seqs + o] = e;
-                        }
+                    uint32_t pe = S.prev_end[csg];
+                    if (i > from) {
+                        const uint2 p = mine[i - 1u < ns ? i - 1u : kSpecCap + (i - 1u - ns)];
+                        pe = (p.x & 0xFFFFu) + (p.x >> 16) + kMinMatch;
+                    }
+                    const uint32_t st0 = e.x & 0xFFFFu, mlm3 = e.x >> 16;
+                    const uint32_t ll = st0 - pe;
+                    cov += mlm3 + kMinMatch;
+                    if constexpr (kRef) {
+                        uint32_t *r = a.ref_seqs + (static_cast<uint64_t>(wi) * a.max_seqs + o) * 3u;
+                        r[0] = ll;
+                        r[1] = mlm3;
+                        r[2] = e.y;
+                    } else {
+                        a.packed[static_cast<uint64_t>(wi) * a.max_seqs + o] = make_uint2(ll | (mlm3 << 16), e.y);
                     }
                 }
                 if (cov) atomicAdd(&S.covered, cov);
             }
             __syncthreads();
-            // start -> literal length: ll(o) = start(o) - end(o-1), chunk by chunk;
-            // every entry is read (and its end shared) before any is rewritten.
-            if (tid == 0) S.carry = 0;
-            for (uint32_t base = 0; base < keep; base += kThreads) {
-                const uint32_t o = base + tid;
-                uint32_t st0 = 0, mlm3 = 0, off = 0;
-                if (o < keep) {
-                    if constexpr (kRef) {
-                        const uint32_t *r = a.ref_seqs + (static_cast<uint64_t>(wi) * a.max_seqs + o) * 3u;
-                        st0 = r[0];
-                        mlm3 = r[1];
-                        off = r[2];
-                    } else {
-                        const uint2 e = a.packed[static_cast<uint64_t>(wi) * a.max_seqs + o];
-                        st0 = e.x & 0xFFFFu;
-                        mlm3 = e.x >> 16;
-                        off = e.y;
-                    }
-                }
-                S.bm[tid] = st0 + mlm3 + kMinMatch;
-                __syncthreads();
-                const uint32_t prev_end = tid ? S.bm[tid - 1] : S.carry;
-                const uint32_t last = (keep - base < kThreads ? keep - base : kThreads) - 1u;
-                const uint32_t next_carry = S.bm[last];
-                if (o < keep) {
-                    const uint32_t ll = st0 - prev_end;
-                    if constexpr (kRef) {
-                        uint32_t *r = a.ref_seqs + (static_cast<uint64_t>(wi) * a.max_seqs + o) * 3u;
-                        r[0] = ll;
-                        r[1] = mlm3;
-                        r[2] = off;
-                    } else {
-                        a.packed[static_cast<uint64_t>(wi) * a.max_seqs + o] = make_uint2(ll | (mlm3 << 16), off);
-                    }
-                }
-                __syncthreads();
-                if (tid == 0) S.carry = next_carry;
-            }
             if (tid == 0) {
                 a.seq_counts[wi] = keep;
                 if (a.lit_counts) a.lit_counts[wi] = size - S.covered;
