@@ -84,7 +84,7 @@ struct SmemLayout {
     uint32_t chain_from[kSegs];
     uint32_t out_off[kSegs];
     uint32_t on_chain[kSegs];
-    uint32_t prev_end[kSegs];  // end of the match before a chain segment's first copied entry
+    uint32_t prev_last[kSegs];  // seg index of the entry before a chain segment's first copied one (~0u: none)
     uint32_t flags;
     uint32_t total;
     uint32_t covered;
@@ -785,19 +785,16 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             // ---- 3. chain walk (one thread), then copy in chain order
             if (tid == 0) {
                 for (uint32_t i = 0; i < kSegs; ++i) S.on_chain[i] = 0;
-                uint32_t cur = 0, from = 0, acc = 0, pend = 0;
+                uint32_t cur = 0, from = 0, acc = 0, last = ~0u;
                 if (lim_pos > 0) {
                     for (;;) {
                         S.on_chain[cur] = 1;
                         S.chain_from[cur] = from;
                         S.out_off[cur] = acc;
-                        S.prev_end[cur] = pend;
+                        S.prev_last[cur] = last;
                         const uint32_t ns = S.spec_count[cur], nc = S.cont_count[cur];
                         acc += (ns - from) + nc;
-                        if (ns + nc > from) {  // the last entry this segment contributes
-                            const uint2 e = seg[cur * kLaneCap + (nc ? kSpecCap + nc - 1u : ns - 1u)];
-                            pend = (e.x & 0xFFFFu) + (e.x >> 16) + kMinMatch;
-                        }
+                        if (ns + nc > from) last = cur * kLaneCap + (nc ? kSpecCap + nc - 1u : ns - 1u);
                         const uint32_t nx = S.sync_warp[cur];
                         if (nx == kNoWarp) break;
                         from = S.sync_idx[cur];
@@ -812,7 +809,7 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             // Write {ll, ml-3, off} in chain order: an entry's literal length is
             // its start minus the end of the entry before it -- the previous
             // entry of the same list, or for a segment's first copied entry the
-            // last entry of the previous chain segment (from the chain walk).
+            // last entry contributed before it, which the chain walk located.
             const uint32_t csg = tid / GL, csl = tid % GL;  // segment whose list this thread copies
             if (S.on_chain[csg]) {
                 const uint32_t from = S.chain_from[csg], ns = S.spec_count[csg], nc = S.cont_count[csg];
@@ -823,10 +820,12 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
                     const uint32_t o = base + (i - from);
                     if (o >= keep) break;
                     const uint2 e = mine[i < ns ? i : kSpecCap + (i - ns)];
-                    uint32_t pe = S.prev_end[csg];
-                    if (i > from) {
-                        const uint2 p = mine[i - 1u < ns ? i - 1u : kSpecCap + (i - 1u - ns)];
-                        pe = (p.x & 0xFFFFu) + (p.x >> 16) + kMinMatch;
+                    const uint32_t pi =
+                        i > from ? csg * kLaneCap + (i - 1u < ns ? i - 1u : kSpecCap + (i - 1u - ns)) : S.prev_last[csg];
+                    uint32_t pe = 0;
+                    if (pi != ~0u) {
+                        const uint32_t px = seg[pi].x;
+                        pe = (px & 0xFFFFu) + (px >> 16) + kMinMatch;
                     }
                     const uint32_t st0 = e.x & 0xFFFFu, mlm3 = e.x >> 16;
                     const uint32_t ll = st0 - pe;
