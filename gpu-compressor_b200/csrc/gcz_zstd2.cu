@@ -431,11 +431,40 @@ __device__ __forceinline__ uint32_t extend_group(const Win &w, uint32_t c, uint3
     return out;
 }
 
+// Bit t (t < 16) set when bytes q+t .. q+t+2 equal bytes q-r+t .. q-r+t+2
+// (zstd_compress.cu:259-275 tests one position at a time).  Both 18-byte
+// ranges are read as aligned words; a byte of x ^ y is zero exactly when its
+// 0x80 flag survives ~(((d & 0x7F..) + 0x7F..) | d | 0x7F..), three flags in
+// a row mark a 3-byte match, and a multiply gathers each word's four flags.
+__device__ __forceinline__ uint32_t rep3_scan16(const Win &w, uint32_t q, uint32_t r) {
+    const uint32_t *wd = reinterpret_cast<const uint32_t *>(w.d - kPre);
+    const uint32_t ax = q + kPre, ay = q - r + kPre;
+    const uint32_t *px = wd + (ax >> 2), *py = wd + (ay >> 2);
+    const uint32_t sx = (ax & 3u) * 8u, sy = (ay & 3u) * 8u;
+    uint32_t z[5];
+    uint32_t xp = px[0], yp = py[0];
+#pragma unroll
+    for (uint32_t j = 0; j < 5; ++j) {
+        const uint32_t xn = px[j + 1], yn = py[j + 1];
+        const uint32_t d = __funnelshift_r(xp, xn, sx) ^ __funnelshift_r(yp, yn, sy);
+        z[j] = ~(((d & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | d | 0x7F7F7F7Fu);
+        xp = xn;
+        yp = yn;
+    }
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t e = z[j] & __funnelshift_r(z[j], z[j + 1], 8) & __funnelshift_r(z[j], z[j + 1], 16);
+        m |= ((e * 0x00204081u) >> 28) << (4u * j);
+    }
+    return m;
+}
+
 // One step of the exact parse for every 8-lane group of the warp at once,
 // each from its own state s (group-uniform); groups with run == false keep
 // theirs.  A group looks at the 32 positions from s.p: the hash-match bits
-// come from the bitmap, and each lane tests the three repeat offsets on four
-// positions (8-byte compares) among those before the first hash match
+// come from the bitmap, and six lanes test the three repeat offsets (16
+// positions each) among those before the first hash match
 // (zstd_compress.cu:259-275).  The first event is the match, extended 32
 // bytes per group iteration, with the lazy step (:278-307) at f+1; with no
 // event the group moves over the 32 positions.  Returns whether the group
@@ -450,39 +479,27 @@ __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, con
     uint32_t H = __funnelshift_r(bm[p >> 5], bm[(p >> 5) + 1], p & 31u);
     if (n32 < 32u) H &= (1u << n32) - 1u;
     const uint32_t nh = H ? static_cast<uint32_t>(__ffs(H)) - 1u : n32;  // positions without a hash match
-    const uint32_t j0 = 4u * gl;
-    const uint32_t q0 = j0 < nh ? p + j0 : p;
-    const uint32_t vlim = j0 < nh ? (nh - j0 < 4u ? nh - j0 : 4u) : 0u;  // positions of this lane to test
-    const uint32_t vall = (1u << vlim) - 1u;
-    uint32_t xlo, xhi;
-    w.u64(static_cast<int>(q0), xlo, xhi);
-    uint32_t mk[3];
-#pragma unroll
-    for (uint32_t k = 0; k < 3; ++k) {
-        const uint32_t rv = k == 0u ? s.r0 : (k == 1u ? s.r1 : s.r2);
-        // positions q0 + t with t < vlim and q0 + t >= rv; their source bytes start at q0 - rv + t >= 0
-        // (rv > q0 only within 3 bytes of a window or segment start)
-        const uint32_t valid = rv <= q0 ? vall : (rv - q0 < vlim ? vall & (~0u << (rv - q0)) : 0u);
-        const int yb = valid ? static_cast<int>(q0) - static_cast<int>(rv) : static_cast<int>(q0);
-        uint32_t ylo, yhi;
-        w.u64(yb, ylo, yhi);
-        const uint32_t dlo = xlo ^ ylo, dhi = xhi ^ yhi;
-        const uint32_t e = ((dlo & 0xFFFFFFu) == 0u ? 1u : 0u) | ((dlo >> 8) == 0u ? 2u : 0u) |
-                           ((__funnelshift_r(dlo, dhi, 16) & 0xFFFFFFu) == 0u ? 4u : 0u) |
-                           ((__funnelshift_r(dlo, dhi, 24) & 0xFFFFFFu) == 0u ? 8u : 0u);
-        mk[k] = e & valid;
-    }
-    const uint32_t any = mk[0] | mk[1] | mk[2];
-    const uint32_t rb = (__ballot_sync(kFull, any != 0u) >> gb) & 0xFFu;
-    const uint32_t l = rb ? static_cast<uint32_t>(__ffs(rb)) - 1u : 0u;
-    const uint32_t al = __shfl_sync(kFull, any, gb + l), m0 = __shfl_sync(kFull, mk[0], gb + l),
-                   m1 = __shfl_sync(kFull, mk[1], gb + l);
-    const bool rep = rb != 0u;
+    // Lane 2k+h (k < 3) tests repeat offset k on the 16 positions from
+    // p + 16h that come before the first hash match and whose source lies in
+    // the window; lanes 6 and 7 test nothing.
+    const uint32_t rk = gl >> 1, hh = gl & 1u;
+    const uint32_t q0 = p + 16u * hh;
+    const uint32_t rv = rk == 0u ? s.r0 : (rk == 1u ? s.r1 : s.r2);
+    const uint32_t lo = rv > q0 ? (rv - q0 < 16u ? rv - q0 : 16u) : 0u;
+    const uint32_t hi = (rk < 3u && nh > 16u * hh) ? (nh - 16u * hh < 16u ? nh - 16u * hh : 16u) : 0u;
+    const uint32_t vm = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+    const uint32_t mk = rep3_scan16(w, q0, rv <= q0 + 16u ? rv : 0u) & vm;
+    const uint32_t mo = __shfl_xor_sync(kFull, mk, 1);
+    const uint32_t mf = hh ? (mo | (mk << 16)) : (mk | (mo << 16));  // offset rk over all 32 positions
+    const uint32_t m0 = __shfl_sync(kFull, mf, gb), m1 = __shfl_sync(kFull, mf, gb + 2u),
+                   m2 = __shfl_sync(kFull, mf, gb + 4u);
+    const uint32_t al = m0 | m1 | m2;
+    const bool rep = al != 0u;
     const bool ev = run && (rep || nh < n32);
     uint32_t f = p + nh, r = 0;
     if (rep) {
         const uint32_t t = static_cast<uint32_t>(__ffs(al)) - 1u;
-        f = p + 4u * l + t;
+        f = p + t;
         r = (m0 >> t) & 1u ? 0u : ((m1 >> t) & 1u ? 1u : 2u);
     }
     const uint32_t fc = ev ? f : 0u;
