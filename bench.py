@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     ap.add_argument("--max-request", type=int, default=256 << 20, help="serving: largest request size")
     ap.add_argument("--max-batch", type=int, default=256 << 20, help="serving: largest batch (bytes of input)")
+    ap.add_argument("--serve-warmup", default="zstd,lzma2", choices=["zstd,lzma2", "lzma2,zstd", "none"],
+                    help="serving: warm-up requests before the stream, in order")
     ap.add_argument("--files", type=int, default=4096, help="uneven: number of files")
     ap.add_argument("--max-file", type=int, default=64 << 20, help="uneven: largest file size")
     return ap.parse_args()
@@ -756,13 +758,16 @@ def fill_pool(pool_np, seed, block=16 << 20):
         list(ex.map(gen, range(nblk)))
 
 
-def measure_serving(ctx, torch, rate, duration, max_request, max_batch, budget=120 * 10**9, pool_bytes=4 << 30):
+def measure_serving(ctx, torch, rate, duration, max_request, max_batch, budget=120 * 10**9, pool_bytes=4 << 30,
+                    warm="zstd,lzma2"):
     """Config 5, serving: an open-loop Poisson stream against the request loop.
     Request sizes log-uniform 4 KiB..max_request, 70% Zstd L1 / 20% Zstd L2 /
     10% LZMA2 L1 (has-match bytes, what the LZMA2 encoder reads).  Payloads are
     slices of a pinned pool made of 16 MiB spans with their own Dirichlet mix;
     results go to a pinned ring freed in completion order.  Reports offered and
-    served GB/s and the submit-to-completion p50/p99 the loop measured."""
+    served GB/s and the submit-to-completion p50/p99 the loop measured.
+    `warm` names the kinds of the warm-up requests, in order ("none": no
+    warm-up, the stream's first requests pay the first launches)."""
     import threading
     import gcz
     from gcz import serving
@@ -822,7 +827,9 @@ def measure_serving(ctx, torch, rate, duration, max_request, max_batch, budget=1
             q[i] = None
             i += 1
 
-    srv.warm_up((serving.ZSTD, serving.LZMA2))
+    kinds_warm = {"zstd": serving.ZSTD, "lzma2": serving.LZMA2}
+    if warm != "none":
+        srv.warm_up(tuple(kinds_warm[k] for k in warm.split(",")))
     base = srv.stats()
     wt = threading.Thread(target=waiter)
     wt.start()
@@ -869,7 +876,7 @@ def measure_serving(ctx, torch, rate, duration, max_request, max_batch, budget=1
         "hbm_budget_bytes": budget, "max_batch_bytes": max_batch, "slots": slots, "device_bytes_held": dev_bytes,
         "batches": st["batches"] - base["batches"], "completed": st["completed"] - base["completed"],
         "submit_seconds": round(t_sub, 3), "wall_s": round(wall, 3), "ring_stalls": rs["stalls"],
-        "max_submit_lag_s": round(late, 4), "status": st["status"]}
+        "max_submit_lag_s": round(late, 4), "warm_up": warm, "status": st["status"]}
 
 
 def run_serving(args):
@@ -881,7 +888,8 @@ def run_serving(args):
     torch.cuda.set_device(local)
     ctx = gcz.Context(local)
     with Clocks(local) as clk:
-        res = measure_serving(ctx, torch, args.rate, args.duration, args.max_request, args.max_batch)
+        res = measure_serving(ctx, torch, args.rate, args.duration, args.max_request, args.max_batch,
+                              warm=args.serve_warmup)
     line = {"metric": "serving input GB/s per B200 (match-find, p50/p99 latency)", "n_gpus": 1,
             "higher_is_better": True, "dtype": "u8", "data": "synthetic (seeded pool)", **res,
             "config": {"workload": "serving_poisson"}, "clocks": clk.summary()}

@@ -117,6 +117,8 @@ struct Win {
         const uint32_t a = static_cast<uint32_t>(q + static_cast<int>(kPre));
         return __funnelshift_r(w[a >> 2], w[(a >> 2) + 1], (a & 3u) * 8u);
     }
+    // The 4 bytes at q, q a multiple of 4.
+    __device__ __forceinline__ uint32_t w32(uint32_t q) const { return reinterpret_cast<const uint32_t *>(d)[q >> 2]; }
     // The 8 bytes at q: three aligned words, two funnel shifts.
     __device__ __forceinline__ void u64(int q, uint32_t &lo, uint32_t &hi) const {
         const uint32_t *w = reinterpret_cast<const uint32_t *>(d - kPre);
@@ -606,24 +608,51 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
         }
         __syncthreads();
         if (S.flags & 2u) return;  // bulk copy never completed: status already recorded, all threads leave
-        const uint32_t nsteps = (size + 31u) >> 5;
-        // Batches of kVB steps per warp: all kVB candidate loads are issued
-        // before any is used, so one memory latency covers the batch.
-        constexpr uint32_t kVB = 8;
-        for (uint32_t b0 = warp * kVB; b0 < kBmWords; b0 += kWarps * kVB) {
-            uint32_t cv[kVB];
+        // Lane l covers positions 4l .. 4l+3 of a 128-position chunk: one
+        // 8-byte load brings its four candidates (2-byte loads where the
+        // window's candidates are not 8-byte aligned or the chunk ends the
+        // window), one aligned 8-byte read its own bytes, and the 8 lanes of
+        // each bitmap word gather their four bits with three shuffles.  kVC
+        // chunks per batch: their candidate loads are all issued first.
+        constexpr uint32_t kChunks = kBmWords / 4u, kVC = 4;
+        static_assert(kBmWords % 4u == 0u, "bitmap words come in 128-position chunks");
+        const bool al8 = (reinterpret_cast<uintptr_t>(cand) & 7u) == 0u;
+        for (uint32_t c0 = warp * kVC; c0 < kChunks; c0 += kWarps * kVC) {
+            uint2 cv[kVC];
 #pragma unroll
-            for (uint32_t u = 0; u < kVB; ++u) {
-                const uint32_t q = (b0 + u) * 32u + lane;
-                cv[u] = (b0 + u < nsteps && q + 3u < size && q > 0u) ? static_cast<uint32_t>(cand[q]) : 0x10000u;
+            for (uint32_t u = 0; u < kVC; ++u) {
+                const uint32_t q = (c0 + u) * 128u + 4u * lane;
+                if (al8 && q + 4u <= size) {
+                    cv[u] = *reinterpret_cast<const uint2 *>(cand + q);
+                } else {
+                    uint32_t e[4];
+#pragma unroll
+                    for (uint32_t k = 0; k < 4; ++k) e[k] = q + k < size ? static_cast<uint32_t>(cand[q + k]) : 0u;
+                    cv[u] = make_uint2(e[0] | (e[1] << 16), e[2] | (e[3] << 16));
+                }
             }
 #pragma unroll
-            for (uint32_t u = 0; u < kVB; ++u) {
-                const uint32_t st = b0 + u;
-                const uint32_t q = st * 32u + lane;
-                const bool hm = cv[u] != 0x10000u && eq3(win, q, zmap(cv[u]));
-                const uint32_t bits = __ballot_sync(kFull, hm);
-                if (lane == 0 && st < kBmWords) S.bm[st] = bits;
+            for (uint32_t u = 0; u < kVC; ++u) {
+                const uint32_t ch = c0 + u;
+                const uint32_t q = ch * 128u + 4u * lane;
+                uint32_t nib = 0;
+                if (q < size) {
+                    const uint32_t x0 = win.w32(q), x1 = win.w32(q + 4u);
+#pragma unroll
+                    for (uint32_t k = 0; k < 4; ++k) {
+                        const uint32_t cw = k < 2u ? cv[u].x : cv[u].y;
+                        const uint32_t c = zmap((k & 1u) ? cw >> 16 : cw & 0xFFFFu);
+                        const uint32_t xk = k ? __funnelshift_r(x0, x1, 8u * k) : x0;
+                        const uint32_t qk = q + k;
+                        const bool hm = qk + 3u < size && qk > 0u && ((xk ^ win.u32(static_cast<int>(c))) & 0xFFFFFFu) == 0u;
+                        nib |= static_cast<uint32_t>(hm) << k;
+                    }
+                }
+                uint32_t v = nib << (4u * (lane & 7u));
+                v |= __shfl_xor_sync(kFull, v, 1);
+                v |= __shfl_xor_sync(kFull, v, 2);
+                v |= __shfl_xor_sync(kFull, v, 4);
+                if ((lane & 7u) == 0u && ch < kChunks) S.bm[ch * 4u + (lane >> 3)] = v;
             }
         }
         __syncthreads();
