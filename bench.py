@@ -282,7 +282,7 @@ def load_tuned(ctx, args):
         if autotune.apply_tuned(ctx) is not None:
             src = "gcz/tuned/" + os.path.basename(autotune.tuned_path(ctx.device))
     ctx.set_option("algo", args.algo)
-    knobs = {k: ctx.query(k) for k in ("algo", "sweep_warps", "sweep_groups", "parse_seg", "parse_ctas",
+    knobs = {k: ctx.query(k) for k in ("algo", "sweep_warps", "sweep_groups", "sweep_prefetch", "parse_seg", "parse_ctas",
                                        "lzma_ctas", "slice_windows")}
     knobs["source"] = src
     return knobs

@@ -75,6 +75,7 @@ struct gcz_ctx {
     int seg_width = 1024;  // Zstd speculative segment: 1024 per 8-lane group, or 2048/4096/8192 per warp
     int sweep_warps = 7;   // candidate-sweep windows per CTA (4-7)
     int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0/1 after a read-back (match_any/ballots), 2/3 one block ahead
+    int sweep_prefetch = 4;  // candidate sweep's L2 prefetch distance of the input, in 128-byte blocks (0, 4, 8)
     int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM
     // profiling
     bool prof = false;
@@ -222,7 +223,7 @@ int zstd_device_core(gcz_ctx *c, Scratch &sc, const uint8_t *d_src, size_t n, ui
     if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(d_src, n, kW, (uint32_t)nb, cand, c->num_sms, st, wins, c->sweep_warps,
-                                           c->sweep_groups));
+                                           c->sweep_groups, c->sweep_prefetch));
         gcz::Zstd2Launch l{};
         l.src = d_src;
         l.cand = cand;
@@ -276,7 +277,7 @@ int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st)
     if (split) {
         uint16_t *cand = static_cast<uint16_t *>(sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(l.src, l.n, l.window, l.num_windows, cand, c->num_sms, st, l.wins,
-                                           c->sweep_warps, c->sweep_groups));
+                                           c->sweep_warps, c->sweep_groups, c->sweep_prefetch));
         gcz::LzmaLaunch lv = l;
         lv.ctas_per_sm = c->lzma_ctas;
         GCZ_CUDA(c, gcz::launch_lzma_verify(lv, cand, st));
@@ -456,6 +457,10 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->sweep_groups = (int)value;
         return GCZ_OK;
     }
+    if (!strcmp(key, "sweep_prefetch") && value >= 0 && value <= 64) {
+        c->sweep_prefetch = (int)value;
+        return GCZ_OK;
+    }
     if (!strcmp(key, "lzma_ctas") && value >= 1 && value <= 8) {
         c->lzma_ctas = (int)value;
         return GCZ_OK;
@@ -490,7 +495,7 @@ extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
         long v;
     } knobs[] = {{"staged", c->staged},          {"parse_ctas", c->parse_ctas},
                  {"parse_seg", c->seg_width},    {"sweep_warps", c->sweep_warps},
-                 {"sweep_groups", c->sweep_groups},
+                 {"sweep_groups", c->sweep_groups}, {"sweep_prefetch", c->sweep_prefetch},
                  {"lzma_ctas", c->lzma_ctas},    {"slice_windows", (long)c->slice_windows},
                  {"frames_slice_windows", (long)c->frames_slice_windows}};
     for (const auto &kv : knobs)
@@ -796,7 +801,7 @@ extern "C" int gcz_zstd_match_find_ref_layout_device(gcz_ctx *c, const uint8_t *
         ProfScope ps(c, st);
         uint16_t *cand = static_cast<uint16_t *>(c->sc.cand.p);
         GCZ_CUDA(c, gcz::launch_cand_sweep(d_input, n_eff, chunk_size, (uint32_t)nb, cand, c->num_sms, st, nullptr,
-                                           c->sweep_warps, c->sweep_groups));
+                                           c->sweep_warps, c->sweep_groups, c->sweep_prefetch));
         gcz::Zstd2Launch l{};
         l.src = d_input;
         l.cand = cand;
@@ -1381,7 +1386,7 @@ int server_launch(gcz_server *sv, ServerSlot &s) {
     if (nb) {
         GCZ_CUDA(c, cudaMemcpyAsync(s.wins.p, s.hwins.data(), nb * sizeof(gcz_window), cudaMemcpyHostToDevice, s.st));
         GCZ_CUDA(c, gcz::launch_cand_sweep(slab_p, slab, kW, (uint32_t)nb, cand, c->num_sms, s.st, dw, c->sweep_warps,
-                                           c->sweep_groups));
+                                           c->sweep_groups, c->sweep_prefetch));
     }
     const uint32_t nz = s.wb[kGrpLzma];  // Zstd windows: sequences and frames groups
     uint64_t *d_off = static_cast<uint64_t *>(s.offsets.p);

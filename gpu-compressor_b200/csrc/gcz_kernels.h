@@ -74,10 +74,12 @@ cudaError_t launch_zstd_match(const ZstdLaunch &l, cudaStream_t st);
 // sweep_warps: windows swept per CTA (4-7, one 32 KiB table each); sweep_groups:
 // lanes with equal hashes in a step grouped by __match_any_sync (0, 2) or by
 // bit-sliced ballots (1, 3), after a table read-back in the blocks that have
-// such lanes (0, 1) or for every step one block ahead (2, 3).  Schedule only.
+// such lanes (0, 1) or for every step one block ahead (2, 3).  sweep_prefetch:
+// in modes 0 and 1, how many 128-byte blocks ahead of the sweep the input is
+// prefetched into L2 (0: none).  Schedule only.
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
                               int num_sms, cudaStream_t st, const WinDesc *wins = nullptr, int sweep_warps = 7,
-                              int sweep_groups = 0);
+                              int sweep_groups = 0, int sweep_prefetch = 0);
 size_t zstd2_seg_scratch_entries(uint32_t num_windows);
 cudaError_t launch_zstd_parse(const Zstd2Launch &l, cudaStream_t st);
 cudaError_t launch_scan_counts(const uint32_t *counts, uint32_t num, uint64_t *offsets, cudaStream_t st);

@@ -51,11 +51,111 @@ __device__ __forceinline__ uint32_t same_key_lanes(uint32_t key, bool valid) {
     return valid ? m : (1u << lane_id());
 }
 
+// One 128-position block of a window's sweep: lane l holds word l of the
+// block (w0) and word l of the next block (w1; only lane 0's is used).
+// The block's hashes (independent of the table): step j, lane l is position
+// blk * 128 + 32 j + l.
+__device__ __forceinline__ void block_hashes(uint32_t blk, uint32_t size, uint32_t w0, uint32_t w1, uint32_t *h,
+                                             bool *v) {
+    const uint32_t lane = lane_id();
+    const uint32_t up = __shfl_down_sync(kFull, w0, 1);
+    const uint32_t n0 = __shfl_sync(kFull, w1, 0);
+    const uint32_t w0n = lane == 31u ? n0 : up;  // word l+1
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t q = blk * 128u + j * 32u + lane;
+        const uint32_t src_lane = j * 8u + (lane >> 2);
+        const uint32_t lo = __shfl_sync(kFull, w0, src_lane);
+        const uint32_t hi = __shfl_sync(kFull, w0n, src_lane);
+        v[j] = q + 3u < size;
+        h[j] = hash4(__funnelshift_r(lo, hi, (lane & 3u) * 8u));
+    }
+}
+
+// The block's table work and candidates, from its hashes.
+template <bool kBallotGroups>
+__device__ __forceinline__ void block_table(uint16_t *T, uint16_t *out, uint32_t blk, uint32_t size,
+                                            const uint32_t *h, const bool *v, uint32_t lt, uint32_t gt) {
+    const uint32_t lane = lane_id();
+    // Step by step: read the bucket, write this position,
+    // read it back.  A lane that does not read back its own position
+    // shares its bucket with another lane of the same step.
+    uint32_t tv[4], dup = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t q = blk * 128u + j * 32u + lane;
+        tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
+        __syncwarp();
+        if (v[j]) T[h[j]] = static_cast<uint16_t>(q);
+        __syncwarp();
+        if (v[j] && T[h[j]] != static_cast<uint16_t>(q)) dup |= 1u << j;
+    }
+    uint32_t g[4] = {1u << lane, 1u << lane, 1u << lane, 1u << lane};
+    const uint32_t dsteps = __reduce_or_sync(kFull, dup);  // steps with equal hashes in two lanes
+    if (dsteps) {
+        // One block in two on compressible data.  Steps before the
+        // first such step j0 wrote each bucket once and are exact.  Put
+        // the table back as it was before j0 (latest steps first, so
+        // each bucket ends with the value its earliest step from j0 on
+        // read) and redo from j0, grouping the lanes of the steps that
+        // share buckets.  Which lanes share a bucket depends only on
+        // the hashes, so the other steps need no groups.
+        const uint32_t j0 = static_cast<uint32_t>(__ffs(dsteps)) - 1u;
+        __syncwarp();
+#pragma unroll
+        for (int j = 3; j >= 0; --j) {
+            if (static_cast<uint32_t>(j) >= j0) {
+                if (v[j]) T[h[j]] = static_cast<uint16_t>(tv[j]);
+                __syncwarp();
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < 4; ++j) {
+            if (j < j0) continue;
+            const uint32_t q = blk * 128u + j * 32u + lane;
+            if ((dsteps >> j) & 1u) {
+                if constexpr (kBallotGroups) g[j] = same_key_lanes<kHashLog>(h[j], v[j]);
+                else g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
+            }
+            tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
+            __syncwarp();
+            if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
+            __syncwarp();
+        }
+    }
+    // ... then the candidates.
+#pragma unroll
+    for (uint32_t j = 0; j < 4; ++j) {
+        const uint32_t q = blk * 128u + j * 32u + lane;
+        const uint32_t lower = g[j] & lt;
+        const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv[j];
+        if (q < size) out[q] = static_cast<uint16_t>(c);
+    }
+}
+
+template <bool kBallotGroups>
+__device__ __forceinline__ void sweep_block(uint16_t *T, uint16_t *out, uint32_t blk, uint32_t size, uint32_t w0,
+                                            uint32_t w1, uint32_t lt, uint32_t gt) {
+    uint32_t h[4];
+    bool v[4];
+    block_hashes(blk, size, w0, w1, h, v);
+    block_table<kBallotGroups>(T, out, blk, size, h, v, lt, gt);
+}
+
+// Word l of block b of a window (0 past its end).
+__device__ __forceinline__ uint32_t block_word(const uint32_t *src32, uint32_t nwords, uint32_t b) {
+    const uint32_t i = b * 32u + lane_id();
+    return i < nwords ? __ldg(src32 + i) : 0u;
+}
+
 // kSweepWarpsPerCta windows per CTA, one 32 KiB table each (7 fill an SM's
 // shared memory); a schedule knob, the candidates do not depend on it.  So is
 // kBallotGroups: how the lanes of a step with equal hashes are grouped
-// (__match_any_sync, or bit-sliced ballots).
-template <int kSweepWarpsPerCta, bool kBallotGroups>
+// (__match_any_sync, or bit-sliced ballots), and kPf, how many 128-byte
+// blocks ahead the input is prefetched into L2 (0: not at all; a compile-time
+// distance, which measured 0.4 ms per GiB faster than the same distance read
+// from the kernel's arguments).
+template <int kSweepWarpsPerCta, bool kBallotGroups, uint32_t kPf>
 __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(SweepArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -72,84 +172,23 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
         const uint32_t *src32 = reinterpret_cast<const uint32_t *>(a.src + start);
         const uint32_t nwords = (size + 3u) >> 2;
         uint16_t *out = a.cand + start;
-        // 128-byte blocks: lane l holds word l.  Two blocks are in flight ahead
-        // of the one being swept, so the load latency stays hidden.
-        uint32_t w0 = lane < nwords ? __ldg(src32 + lane) : 0u;
-        uint32_t w1 = 32u + lane < nwords ? __ldg(src32 + 32u + lane) : 0u;
-        for (uint32_t blk = 0; blk * 128u < size; ++blk) {
-            const uint32_t nw = (blk + 2u) * 32u + lane;
-            const uint32_t w2 = nw < nwords ? __ldg(src32 + nw) : 0u;
-            const uint32_t up = __shfl_down_sync(kFull, w0, 1);
-            const uint32_t n0 = __shfl_sync(kFull, w1, 0);
-            const uint32_t w0n = lane == 31u ? n0 : up;  // word l+1
-            // Hashes of the 4 steps first (independent of the table) ...
-            uint32_t h[4];
-            bool v[4];
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t q = blk * 128u + j * 32u + lane;
-                const uint32_t src_lane = j * 8u + (lane >> 2);
-                const uint32_t lo = __shfl_sync(kFull, w0, src_lane);
-                const uint32_t hi = __shfl_sync(kFull, w0n, src_lane);
-                v[j] = q + 3u < size;
-                h[j] = hash4(__funnelshift_r(lo, hi, (lane & 3u) * 8u));
-            }
-            // ... then, step by step: read the bucket, write this position,
-            // read it back.  A lane that does not read back its own position
-            // shares its bucket with another lane of the same step.
-            uint32_t tv[4], dup = 0;
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t q = blk * 128u + j * 32u + lane;
-                tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
-                __syncwarp();
-                if (v[j]) T[h[j]] = static_cast<uint16_t>(q);
-                __syncwarp();
-                if (v[j] && T[h[j]] != static_cast<uint16_t>(q)) dup |= 1u << j;
-            }
-            uint32_t g[4] = {1u << lane, 1u << lane, 1u << lane, 1u << lane};
-            const uint32_t dsteps = __reduce_or_sync(kFull, dup);  // steps with equal hashes in two lanes
-            if (dsteps) {
-                // One block in two on compressible data.  Steps before the
-                // first such step j0 wrote each bucket once and are exact.  Put
-                // the table back as it was before j0 (latest steps first, so
-                // each bucket ends with the value its earliest step from j0 on
-                // read) and redo from j0, grouping the lanes of the steps that
-                // share buckets.  Which lanes share a bucket depends only on
-                // the hashes, so the other steps need no groups.
-                const uint32_t j0 = static_cast<uint32_t>(__ffs(dsteps)) - 1u;
-                __syncwarp();
-#pragma unroll
-                for (int j = 3; j >= 0; --j) {
-                    if (static_cast<uint32_t>(j) >= j0) {
-                        if (v[j]) T[h[j]] = static_cast<uint16_t>(tv[j]);
-                        __syncwarp();
-                    }
+        const uint32_t nblk = (size + 127u) >> 7;
+        {
+            // 128-byte blocks: lane l holds word l.  Each block's words are
+            // loaded two blocks ahead of its sweep; with kPf > 0 lane 0 also
+            // prefetches block b + kPf into L2 while block b is swept, so that
+            // those loads hit L2 instead of waiting on DRAM.
+            uint32_t w0 = block_word(src32, nwords, 0), w1 = block_word(src32, nwords, 1);
+            for (uint32_t blk = 0; blk < nblk; ++blk) {
+                if constexpr (kPf > 0) {
+                    const uint32_t pw = (blk + kPf) * 32u;
+                    if (lane == 0 && pw < nwords) asm volatile("prefetch.global.L2 [%0];" ::"l"(src32 + pw));
                 }
-#pragma unroll
-                for (uint32_t j = 0; j < 4; ++j) {
-                    if (j < j0) continue;
-                    const uint32_t q = blk * 128u + j * 32u + lane;
-                    if ((dsteps >> j) & 1u) {
-                        if constexpr (kBallotGroups) g[j] = same_key_lanes<kHashLog>(h[j], v[j]);
-                        else g[j] = __match_any_sync(kFull, v[j] ? h[j] : (0x80000000u | lane));
-                    }
-                    tv[j] = v[j] ? static_cast<uint32_t>(T[h[j]]) : 0xFFFFu;
-                    __syncwarp();
-                    if (v[j] && !(g[j] & gt)) T[h[j]] = static_cast<uint16_t>(q);
-                    __syncwarp();
-                }
+                const uint32_t w2 = block_word(src32, nwords, blk + 2u);
+                sweep_block<kBallotGroups>(T, out, blk, size, w0, w1, lt, gt);
+                w0 = w1;
+                w1 = w2;
             }
-            // ... then the candidates.
-#pragma unroll
-            for (uint32_t j = 0; j < 4; ++j) {
-                const uint32_t q = blk * 128u + j * 32u + lane;
-                const uint32_t lower = g[j] & lt;
-                const uint32_t c = lower ? (q - lane + 31u - static_cast<uint32_t>(__clz(lower))) : tv[j];
-                if (q < size) out[q] = static_cast<uint16_t>(c);
-            }
-            w0 = w1;
-            w1 = w2;
         }
         __syncwarp();
     }
@@ -164,8 +203,8 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
 // take the next lower lane's position) and one write (the highest lane of each
 // group), with no read-back and no redo.
 template <bool kBallots>
-__device__ __forceinline__ void block_hashes(uint32_t blk, uint32_t size, uint32_t w0, uint32_t w1, uint32_t *h,
-                                             bool *v, uint32_t *g) {
+__device__ __forceinline__ void block_hashes_groups(uint32_t blk, uint32_t size, uint32_t w0, uint32_t w1,
+                                                    uint32_t *h, bool *v, uint32_t *g) {
     const uint32_t lane = lane_id();
     const uint32_t up = __shfl_down_sync(kFull, w0, 1);
     const uint32_t n0 = __shfl_sync(kFull, w1, 0);
@@ -207,14 +246,14 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_ahead_kerne
         uint32_t w1 = 32u + lane < nwords ? __ldg(src32 + 32u + lane) : 0u;
         uint32_t h[4], g[4];
         bool v[4];
-        block_hashes<kBallots>(0u, size, w0, w1, h, v, g);
+        block_hashes_groups<kBallots>(0u, size, w0, w1, h, v, g);
         for (uint32_t blk = 0; blk * 128u < size; ++blk) {
             const uint32_t nw = (blk + 2u) * 32u + lane;
             const uint32_t w2 = nw < nwords ? __ldg(src32 + nw) : 0u;
             // the next block's hashes and groups: no dependence on the table
             uint32_t hn[4], gn[4];
             bool vn[4];
-            block_hashes<kBallots>(blk + 1u, size, w1, w2, hn, vn, gn);
+            block_hashes_groups<kBallots>(blk + 1u, size, w1, w2, hn, vn, gn);
 #pragma unroll
             for (uint32_t j = 0; j < 4; ++j) {
                 const uint32_t q = blk * 128u + j * 32u + lane;
@@ -242,10 +281,11 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_ahead_kerne
 }  // namespace
 
 namespace {
-template <int kWarps, int kMode>
+template <int kWarps, int kMode, uint32_t kPf = 0>
 cudaError_t launch_sweep_variant(const SweepArgs &a, int num_sms, cudaStream_t st) {
     constexpr bool kBallots = (kMode & 1) != 0, kAhead = kMode >= 2;
-    const auto kernel = kAhead ? cand_sweep_ahead_kernel<kWarps, kBallots> : cand_sweep_kernel<kWarps, kBallots>;
+    const auto kernel =
+        kAhead ? cand_sweep_ahead_kernel<kWarps, kBallots> : cand_sweep_kernel<kWarps, kBallots, kAhead ? 0u : kPf>;
     const uint32_t smem = kWarps * kHashSize * sizeof(uint16_t);
     static SmemOnce smem_set{0};
     cudaError_t e = set_smem_once(kernel, smem, smem_set);
@@ -261,20 +301,26 @@ cudaError_t launch_sweep_variant(const SweepArgs &a, int num_sms, cudaStream_t s
 }  // namespace
 
 cudaError_t launch_cand_sweep(const uint8_t *src, uint64_t n, uint32_t window, uint32_t num_windows, uint16_t *cand,
-                              int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps, int sweep_groups) {
+                              int num_sms, cudaStream_t st, const WinDesc *wins, int sweep_warps, int sweep_groups,
+                              int sweep_prefetch) {
     if (num_windows == 0) return cudaSuccess;
     SweepArgs a{src, n, window, num_windows, cand, wins};
     // sweep_groups: 0 / 1 group equal-hash lanes (__match_any_sync / ballots)
     // only in blocks that need it, after a read-back; 2 / 3 form every step's
-    // groups one block ahead.
-    switch (sweep_groups * 8 + sweep_warps) {
-#define GCZ_SWEEP_CASE(M, W) \
-    case M * 8 + W: return launch_sweep_variant<W, M>(a, num_sms, st);
-#define GCZ_SWEEP_MODE(M) GCZ_SWEEP_CASE(M, 4) GCZ_SWEEP_CASE(M, 5) GCZ_SWEEP_CASE(M, 6) GCZ_SWEEP_CASE(M, 7)
-        GCZ_SWEEP_MODE(0) GCZ_SWEEP_MODE(1) GCZ_SWEEP_MODE(2) GCZ_SWEEP_MODE(3)
+    // groups one block ahead.  sweep_prefetch: the read-back modes' L2
+    // prefetch distance of the input, 0, 4 or 8 128-byte blocks (other values
+    // are rounded down to one of these).
+    const int pf = sweep_groups >= 2 ? 0 : (sweep_prefetch >= 8 ? 2 : (sweep_prefetch >= 4 ? 1 : 0));
+    switch ((pf * 4 + sweep_groups) * 8 + sweep_warps) {
+#define GCZ_SWEEP_CASE(P, M, W) \
+    case (P * 4 + M) * 8 + W: return launch_sweep_variant<W, M, P * 4u>(a, num_sms, st);
+#define GCZ_SWEEP_MODE(P, M) \
+    GCZ_SWEEP_CASE(P, M, 4) GCZ_SWEEP_CASE(P, M, 5) GCZ_SWEEP_CASE(P, M, 6) GCZ_SWEEP_CASE(P, M, 7)
+        GCZ_SWEEP_MODE(0, 0) GCZ_SWEEP_MODE(0, 1) GCZ_SWEEP_MODE(0, 2) GCZ_SWEEP_MODE(0, 3)
+        GCZ_SWEEP_MODE(1, 0) GCZ_SWEEP_MODE(1, 1) GCZ_SWEEP_MODE(2, 0) GCZ_SWEEP_MODE(2, 1)
 #undef GCZ_SWEEP_MODE
 #undef GCZ_SWEEP_CASE
-    default: return launch_sweep_variant<7, 0>(a, num_sms, st);
+    default: return launch_sweep_variant<7, 0, 8u>(a, num_sms, st);
     }
 }
 

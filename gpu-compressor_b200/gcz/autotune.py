@@ -8,6 +8,8 @@ scheduled:
          "sweep_groups" the sweep's grouping of lanes that share a hash bucket:
                         after a read-back (0: __match_any_sync, 1: ballots) or
                         one block ahead for every step (2, 3 likewise)
+         "sweep_prefetch" how far ahead (0, 4 or 8 blocks of 128 bytes) the
+                        read-back sweeps prefetch their input into L2
          "parse_seg"    speculative segment of the second stage: 2048, 4096 or
                         8192 bytes per warp (32, 16 or 8 warps per window), or
                         1024 bytes per 8-lane group (64 segments per window)
@@ -36,9 +38,9 @@ TUNED_DIR = os.path.join(HERE, "tuned")
 # slower on every input measured, and "algo" also switches LZMA2's kernels, so
 # the search stays within the split kernels.
 ZSTD_CANDIDATES = [
-    {"algo": 2, "sweep_warps": sw, "sweep_groups": sg, "parse_seg": seg, "parse_ctas": ctas}
+    {"algo": 2, "sweep_warps": sw, "sweep_groups": sg, "sweep_prefetch": pf, "parse_seg": seg, "parse_ctas": ctas}
     for sw in (7, 6, 5, 4)
-    for sg in (0, 1, 2, 3)
+    for sg, pf in ((0, 4), (0, 8), (0, 0), (1, 4), (1, 0), (2, 0), (3, 0))
     for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (8192, (3, 2)), (2048, (1,)))
     for ctas in ctas_list
 ]

@@ -82,6 +82,8 @@ const char *gcz_version(void);
  * that share a hash bucket: after a table read-back, only in blocks that have
  * such lanes, with __match_any_sync (0, default) or bit-sliced ballots (1), or
  * for every step one block ahead of the table work (2, 3 likewise);
+ * "sweep_prefetch" = how many 128-byte blocks ahead of itself the read-back
+ * sweep (groups 0, 1) prefetches its input into L2: 0, 4 (default) or 8;
  * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
  * default 3); "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 512 = 32 MiB; four slots, three slices in flight;

@@ -76,27 +76,32 @@ def test_compact_host_api_matches_oracle(ctx, name, spec):
     np.testing.assert_array_equal(seqs, o_seqs)
 
 
-@pytest.mark.parametrize("algo,seg,sweep", [(2, 4096, 0), (2, 1024, 0), (2, 1024, 1), (2, 1024, 2), (2, 1024, 3),
-                                             (1, 4096, 0)],
-                         ids=["split", "split-group1k", "sweep-ballots", "sweep-ahead", "sweep-ahead-ballots", "fused"])
+@pytest.mark.parametrize("algo,seg,sweep,pf", [(2, 4096, 0, 4), (2, 1024, 0, 4), (2, 1024, 0, 0), (2, 1024, 0, 8),
+                                                (2, 1024, 1, 4), (2, 1024, 1, 0), (2, 1024, 2, 0), (2, 1024, 3, 0),
+                                                (1, 4096, 0, 4)],
+                         ids=["split", "split-group1k", "sweep-no-prefetch", "sweep-prefetch8", "sweep-ballots",
+                              "sweep-ballots-no-prefetch", "sweep-ahead", "sweep-ahead-ballots", "fused"])
 @pytest.mark.parametrize("seed,n,mix", [(1, 16 << 20, (0.4, 0.4, 0.2)), (31, 5 << 20, (0.05, 0.9, 0.05)),
                                         (32, 3 << 20 | 12345, (0.9, 0.05, 0.05)), (33, 2 << 20, (0.0, 0.0, 1.0)),
                                         (34, 2 << 20, (0.0, 1.0, 0.0))])
-def test_synthetic_vs_oracle(ctx, seed, n, mix, algo, seg, sweep):
+def test_synthetic_vs_oracle(ctx, seed, n, mix, algo, seg, sweep, pf):
     """Zstd L1 plain workload shape (16 MiB, seed 1) and skewed mixes, over the
-    kernel families, segment layouts and sweep groupings."""
+    kernel families, segment layouts, sweep groupings and sweep prefetch
+    distances."""
     import gcz
 
     data = gcz.gen_synthetic(seed, n, 8 << 20, mix)
     ctx.set_option("algo", algo)
     ctx.set_option("parse_seg", seg)
     ctx.set_option("sweep_groups", sweep)
+    ctx.set_option("sweep_prefetch", pf)
     try:
         seqs, offsets = ctx.zstd_match_find(data, 16)
     finally:
         ctx.set_option("algo", 2)
         ctx.set_option("parse_seg", 1024)
         ctx.set_option("sweep_groups", 0)
+        ctx.set_option("sweep_prefetch", 4)
     o_seqs, o_off = orc.zstd_sequences(data, 16, threads=16)
     np.testing.assert_array_equal(offsets, o_off)
     np.testing.assert_array_equal(seqs, o_seqs)
