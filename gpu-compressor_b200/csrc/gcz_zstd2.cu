@@ -481,6 +481,12 @@ __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, con
     uint32_t H = __funnelshift_r(bm[p >> 5], bm[(p >> 5) + 1], p & 31u);
     if (n32 < 32u) H &= (1u << n32) - 1u;
     const uint32_t nh = H ? static_cast<uint32_t>(__ffs(H)) - 1u : n32;  // positions without a hash match
+    // The candidates at the first hash match and the position after it are
+    // loaded before the repeat-offset test, so that their latency overlaps
+    // it: the event is that hash match unless a repeat offset hits earlier
+    // (a few times per window), and only then is cand(f+1) loaded again.
+    const uint32_t fh = nh < n32 ? p + nh : 0u;
+    const uint32_t ch0 = cand[fh], ch1 = cand[fh + 1u];
     // Lane 2k+h (k < 3) tests repeat offset k on the 16 positions from
     // p + 16h that come before the first hash match and whose source lies in
     // the window; lanes 6 and 7 test nothing.
@@ -505,7 +511,9 @@ __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, con
         r = (m0 >> t) & 1u ? 0u : ((m1 >> t) & 1u ? 1u : 2u);
     }
     const uint32_t fc = ev ? f : 0u;
-    const uint32_t cf = zmap(cand[fc]), cf1 = zmap(cand[fc + 1u]);
+    const uint32_t cf = zmap(ch0);
+    uint32_t cf1 = zmap(ch1);
+    if (rep) cf1 = zmap(cand[fc + 1u]);
     uint32_t off, c0;
     if (!rep) {
         off = fc - cf;
