@@ -445,7 +445,7 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->parse_ctas = (int)value;
         return GCZ_OK;
     }
-    if (!strcmp(key, "parse_seg") && (value == 1024 || value == 2048 || value == 4096 || value == 8192)) {
+    if (!strcmp(key, "parse_seg") && (value == 512 || value == 1024 || value == 2048 || value == 4096 || value == 8192)) {
         c->seg_width = (int)value;
         return GCZ_OK;
     }

@@ -48,8 +48,10 @@ namespace {
 
 constexpr uint32_t kMinMatch = 3;                 // MIN_MATCH_LEN, zstd_compress.cu:28
 // Speculative segment width is a schedule knob: 2, 4 or 8 KiB parsed by one
-// warp each (32, 16 or 8 warps per window), or 1 KiB parsed by an 8-lane group
-// (four segments per warp, 64 per window).  It never changes the sequences.
+// warp each (32, 16 or 8 warps per window), 1 KiB parsed by an 8-lane group
+// (four segments per warp, 64 per window), or 512 bytes parsed by a 4-lane
+// group (eight segments per warp, 128 per window).  It never changes the
+// sequences.
 template <uint32_t SegW, uint32_t GL = 32>
 struct SegCfg {
     static constexpr uint32_t kSegW = SegW;
@@ -63,11 +65,15 @@ struct SegCfg {
     // written in 32-entry blocks.
     static constexpr uint32_t kLook = GL == 32 ? 128 : 32;
     static constexpr uint32_t kSpecCap = ((SegW + kLook) / 3 + 1 + 31) / 32 * 32;
-    static constexpr uint32_t kContCap = GL == 32 ? 256 : 128;  // continuation matches before giving up
+    // continuation matches before giving up (a guessed parse meets the true
+    // one after ~3 matches; the cap keeps every layout's lists within the
+    // 1 KiB layout's 32768 entries per window)
+    static constexpr uint32_t kContCap = GL == 32 ? 256 : (GL == 8 ? 128 : 64);
     static constexpr uint32_t kLaneCap = kSpecCap + kContCap;
     static constexpr uint32_t kMinBlocks = kThreads >= 1024 ? 1 : 3;
 };
 constexpr uint32_t kNoWarp = 0xFFFFu;
+constexpr uint32_t kNoEntry = 0xFFFFu;
 
 constexpr uint32_t kPre = 64;                           // zero bytes before the window
 constexpr uint32_t kDataBytes = kPre + kMaxWindow + 64; // + zero pad after it
@@ -77,14 +83,17 @@ template <uint32_t kSegs>
 struct SmemLayout {
     uint8_t data[kDataBytes];
     uint32_t bm[kBmWords];
-    uint32_t spec_count[kSegs];
-    uint32_t cont_count[kSegs];
-    uint32_t sync_warp[kSegs];
-    uint32_t sync_idx[kSegs];
-    uint32_t chain_from[kSegs];
-    uint32_t out_off[kSegs];
-    uint32_t on_chain[kSegs];
-    uint32_t prev_last[kSegs];  // seg index of the entry before a chain segment's first copied one (~0u: none)
+    // Per segment, 16 bits each (list lengths, indices and output offsets of
+    // a window are below 2^15; segment indices below 2^7), so that 128
+    // segments fit beside the window at three CTAs per SM.
+    uint16_t spec_count[kSegs];
+    uint16_t cont_count[kSegs];
+    uint16_t sync_warp[kSegs];
+    uint16_t sync_idx[kSegs];
+    uint16_t chain_from[kSegs];
+    uint16_t out_off[kSegs];
+    uint16_t on_chain[kSegs];
+    uint16_t prev_last[kSegs];  // seg index of the entry before a chain segment's first copied one (kNoEntry: none)
     uint32_t flags;
     uint32_t total;
     uint32_t covered;
@@ -462,18 +471,46 @@ __device__ __forceinline__ uint32_t rep3_scan16(const Win &w, uint32_t q, uint32
     return m;
 }
 
-// One step of the exact parse for every 8-lane group of the warp at once,
-// each from its own state s (group-uniform); groups with run == false keep
-// theirs.  A group looks at the 32 positions from s.p: the hash-match bits
-// come from the bitmap, and six lanes test the three repeat offsets (16
-// positions each) among those before the first hash match
-// (zstd_compress.cu:259-275).  The first event is the match, extended 32
-// bytes per group iteration, with the lazy step (:278-307) at f+1; with no
-// event the group moves over the 32 positions.  Returns whether the group
-// found a match (m set, s advanced past it, repeat offsets updated).
+// Bit t (t < 32) set when bytes q+t .. q+t+2 equal bytes q-r+t .. q-r+t+2:
+// rep3_scan16 over 32 positions (34-byte ranges, ten aligned words each).
+__device__ __forceinline__ uint32_t rep3_scan32(const Win &w, uint32_t q, uint32_t r) {
+    const uint32_t *wd = reinterpret_cast<const uint32_t *>(w.d - kPre);
+    const uint32_t ax = q + kPre, ay = q - r + kPre;
+    const uint32_t *px = wd + (ax >> 2), *py = wd + (ay >> 2);
+    const uint32_t sx = (ax & 3u) * 8u, sy = (ay & 3u) * 8u;
+    uint32_t z[9];
+    uint32_t xp = px[0], yp = py[0];
+#pragma unroll
+    for (uint32_t j = 0; j < 9; ++j) {
+        const uint32_t xn = px[j + 1], yn = py[j + 1];
+        const uint32_t d = __funnelshift_r(xp, xn, sx) ^ __funnelshift_r(yp, yn, sy);
+        z[j] = ~(((d & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | d | 0x7F7F7F7Fu);
+        xp = xn;
+        yp = yn;
+    }
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < 8; ++j) {
+        const uint32_t e = z[j] & __funnelshift_r(z[j], z[j + 1], 8) & __funnelshift_r(z[j], z[j + 1], 16);
+        m |= ((e * 0x00204081u) >> 28) << (4u * j);
+    }
+    return m;
+}
+
+// One step of the exact parse for every GL-lane group of the warp at once
+// (GL = 8 or 4), each from its own state s (group-uniform); groups with
+// run == false keep theirs.  A group looks at the 32 positions from s.p: the
+// hash-match bits come from the bitmap, and the lanes test the three repeat
+// offsets among the positions before the first hash match
+// (zstd_compress.cu:259-275) -- six lanes of 16 positions each (GL = 8) or
+// three of 32 (GL = 4).  The first event is the match, extended 8 * GL bytes
+// per group iteration, with the lazy step (:278-307) at f+1; with no event
+// the group moves over the 32 positions.  Returns whether the group found a
+// match (m set, s advanced past it, repeat offsets updated).
+template <uint32_t GL>
 __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, const uint16_t *cand, uint32_t size,
                                            bool lazy, bool run, PState &s, Match &m) {
-    constexpr uint32_t GL = 8;
+    static_assert(GL == 8 || GL == 4, "8- or 4-lane groups");
     const uint32_t lane = lane_id(), gl = lane & (GL - 1u), gb = lane & ~(GL - 1u);
     const uint32_t p = run ? s.p : 0u;
     const uint32_t lim = run ? size - 3u - p : 0u;
@@ -487,20 +524,36 @@ __device__ __forceinline__ bool group_step(const Win &w, const uint32_t *bm, con
     // (a few times per window), and only then is cand(f+1) loaded again.
     const uint32_t fh = nh < n32 ? p + nh : 0u;
     const uint32_t ch0 = cand[fh], ch1 = cand[fh + 1u];
-    // Lane 2k+h (k < 3) tests repeat offset k on the 16 positions from
-    // p + 16h that come before the first hash match and whose source lies in
-    // the window; lanes 6 and 7 test nothing.
-    const uint32_t rk = gl >> 1, hh = gl & 1u;
-    const uint32_t q0 = p + 16u * hh;
-    const uint32_t rv = rk == 0u ? s.r0 : (rk == 1u ? s.r1 : s.r2);
-    const uint32_t lo = rv > q0 ? (rv - q0 < 16u ? rv - q0 : 16u) : 0u;
-    const uint32_t hi = (rk < 3u && nh > 16u * hh) ? (nh - 16u * hh < 16u ? nh - 16u * hh : 16u) : 0u;
-    const uint32_t vm = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
-    const uint32_t mk = rep3_scan16(w, q0, rv <= q0 + 16u ? rv : 0u) & vm;
-    const uint32_t mo = __shfl_xor_sync(kFull, mk, 1);
-    const uint32_t mf = hh ? (mo | (mk << 16)) : (mk | (mo << 16));  // offset rk over all 32 positions
-    const uint32_t m0 = __shfl_sync(kFull, mf, gb), m1 = __shfl_sync(kFull, mf, gb + 2u),
-                   m2 = __shfl_sync(kFull, mf, gb + 4u);
+    uint32_t m0, m1, m2;  // per repeat offset: hits among the 32 positions
+    if constexpr (GL == 8) {
+        // Lane 2k+h (k < 3) tests repeat offset k on the 16 positions from
+        // p + 16h that come before the first hash match and whose source lies
+        // in the window; lanes 6 and 7 test nothing.
+        const uint32_t rk = gl >> 1, hh = gl & 1u;
+        const uint32_t q0 = p + 16u * hh;
+        const uint32_t rv = rk == 0u ? s.r0 : (rk == 1u ? s.r1 : s.r2);
+        const uint32_t lo = rv > q0 ? (rv - q0 < 16u ? rv - q0 : 16u) : 0u;
+        const uint32_t hi = (rk < 3u && nh > 16u * hh) ? (nh - 16u * hh < 16u ? nh - 16u * hh : 16u) : 0u;
+        const uint32_t vm = ((1u << hi) - 1u) & ~((1u << lo) - 1u);
+        const uint32_t mk = rep3_scan16(w, q0, rv <= q0 + 16u ? rv : 0u) & vm;
+        const uint32_t mo = __shfl_xor_sync(kFull, mk, 1);
+        const uint32_t mf = hh ? (mo | (mk << 16)) : (mk | (mo << 16));  // offset rk over all 32 positions
+        m0 = __shfl_sync(kFull, mf, gb);
+        m1 = __shfl_sync(kFull, mf, gb + 2u);
+        m2 = __shfl_sync(kFull, mf, gb + 4u);
+    } else {
+        // Lane k (k < 3) tests repeat offset k on the 32 positions from p
+        // that come before the first hash match and whose source lies in the
+        // window; lane 3 tests nothing.
+        const uint32_t rv = gl == 0u ? s.r0 : (gl == 1u ? s.r1 : s.r2);
+        const uint32_t lo = rv > p ? (rv - p < 32u ? rv - p : 32u) : 0u;
+        const uint32_t hi = gl < 3u ? nh : 0u;  // nh <= 32
+        const uint32_t vm = (hi >= 32u ? ~0u : (1u << hi) - 1u) & (lo >= 32u ? 0u : ~((1u << lo) - 1u));
+        const uint32_t mk = rep3_scan32(w, p, rv <= p + 32u ? rv : 0u) & vm;
+        m0 = __shfl_sync(kFull, mk, gb);
+        m1 = __shfl_sync(kFull, mk, gb + 1u);
+        m2 = __shfl_sync(kFull, mk, gb + 2u);
+    }
     const uint32_t al = m0 | m1 | m2;
     const bool rep = al != 0u;
     const bool ev = run && (rep || nh < n32);
@@ -756,7 +809,7 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
                 const bool run = active && s.p < stop && s.p + 3u < size;
                 if (!__any_sync(kFull, run)) break;
                 Match m;
-                if (group_step(win, S.bm, cand, size, lazy, run, s, m)) {
+                if (group_step<GL>(win, S.bm, cand, size, lazy, run, s, m)) {
                     if (gl == 0) lst[n] = pack_entry(m);
                     ++n;
                 }
@@ -777,7 +830,7 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
                 const bool run = crun && s.p + 3u < size;
                 if (!__any_sync(kFull, run)) break;
                 Match m;
-                const bool ev = group_step(win, S.bm, cand, size, lazy, run, s, m);
+                const bool ev = group_step<GL>(win, S.bm, cand, size, lazy, run, s, m);
                 uint32_t tcount = 0;
                 const uint2 *tl = seg;
                 if (ev) {
@@ -839,7 +892,7 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             // ---- 3. chain walk (one thread), then copy in chain order
             if (tid == 0) {
                 for (uint32_t i = 0; i < kSegs; ++i) S.on_chain[i] = 0;
-                uint32_t cur = 0, from = 0, acc = 0, last = ~0u;
+                uint32_t cur = 0, from = 0, acc = 0, last = kNoEntry;
                 if (lim_pos > 0) {
                     for (;;) {
                         S.on_chain[cur] = 1;
@@ -877,7 +930,7 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
                     const uint32_t pi =
                         i > from ? csg * kLaneCap + (i - 1u < ns ? i - 1u : kSpecCap + (i - 1u - ns)) : S.prev_last[csg];
                     uint32_t pe = 0;
-                    if (pi != ~0u) {
+                    if (pi != kNoEntry) {
                         const uint32_t px = seg[pi].x;
                         pe = (px & 0xFFFFu) + (px >> 16) + kMinMatch;
                     }
@@ -945,6 +998,7 @@ constexpr uint32_t kSegStride = []() constexpr {
     if (seg_entries<4096>() > m) m = seg_entries<4096>();
     if (seg_entries<8192>() > m) m = seg_entries<8192>();
     if (seg_entries<1024, 8>() > m) m = seg_entries<1024, 8>();
+    if (seg_entries<512, 4>() > m) m = seg_entries<512, 4>();
     return m;
 }();
 
@@ -967,6 +1021,7 @@ cudaError_t launch_parse_variant(const Zstd2Args &a, int num_sms, int ctas_per_s
 
 template <bool kRef>
 cudaError_t launch_parse_ref(const Zstd2Args &a, uint32_t seg_width, int num_sms, int ctas_per_sm, cudaStream_t st) {
+    if (seg_width == 512) return launch_parse_variant<kRef, 512, 4>(a, num_sms, ctas_per_sm, st);
     if (seg_width == 1024) return launch_parse_variant<kRef, 1024, 8>(a, num_sms, ctas_per_sm, st);
     if (seg_width == 2048) return launch_parse_variant<kRef, 2048, 32>(a, num_sms, ctas_per_sm, st);
     if (seg_width == 8192) return launch_parse_variant<kRef, 8192, 32>(a, num_sms, ctas_per_sm, st);

@@ -12,7 +12,8 @@ scheduled:
                         read-back sweeps prefetch their input into L2
          "parse_seg"    speculative segment of the second stage: 2048, 4096 or
                         8192 bytes per warp (32, 16 or 8 warps per window), or
-                        1024 bytes per 8-lane group (64 segments per window)
+                        1024 bytes per 8-lane group (64 segments per window),
+                        or 512 bytes per 4-lane group (128 segments)
          "parse_ctas"   second-stage CTAs per SM
   LZMA2  "lzma_ctas"    second-stage CTAs per SM (the sweep is shared)
   host   "slice_windows" windows per slice of the host-buffer pipelines
@@ -41,7 +42,7 @@ ZSTD_CANDIDATES = [
     {"algo": 2, "sweep_warps": sw, "sweep_groups": sg, "sweep_prefetch": pf, "parse_seg": seg, "parse_ctas": ctas}
     for sw in (7, 6, 5, 4)
     for sg, pf in ((0, 4), (0, 8), (0, 0), (1, 4), (1, 0), (2, 0), (3, 0))
-    for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (8192, (3, 2)), (2048, (1,)))
+    for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (512, (3, 2)), (8192, (3, 2)), (2048, (1,)))
     for ctas in ctas_list
 ]
 LZMA_CANDIDATES = [{"lzma_ctas": c} for c in (3, 2, 1)]

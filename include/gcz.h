@@ -76,8 +76,8 @@ const char *gcz_version(void);
  * single-warp kernels; "staged" (algo 1) = 1 stages each window into shared
  * memory with bulk copies, 0 reads it through L1; "parse_ctas" = Zstd
  * second-stage CTAs per SM (1-8); "parse_seg" = the Zstd second stage's
- * speculative segment: 1024 bytes per 8-lane group (default), or 2048, 4096
- * or 8192 bytes per warp; "sweep_warps" = windows per candidate-sweep CTA
+ * speculative segment: 1024 bytes per 8-lane group (default), 512 bytes per
+ * 4-lane group, or 2048, 4096 or 8192 bytes per warp; "sweep_warps" = windows per candidate-sweep CTA
  * (4-7, default 7); "sweep_groups" = how the sweep groups the lanes of a step
  * that share a hash bucket: after a table read-back, only in blocks that have
  * such lanes, with __match_any_sync (0, default) or bit-sliced ballots (1), or

@@ -39,9 +39,10 @@ def run_ref_layout(ctx, data, window, depth, max_seqs):
             sc.cpu().numpy().view(np.uint32)[:B], lc.cpu().numpy().view(np.uint32)[:B])
 
 
-@pytest.mark.parametrize("algo,staged,seg", [(2, 1, 4096), (2, 1, 1024), (2, 1, 2048), (2, 1, 8192), (1, 1, 4096),
-                                             (1, 0, 4096)],
-                         ids=["split", "split-group1k", "split-seg2k", "split-seg8k", "fused-staged", "fused-l1"])
+@pytest.mark.parametrize("algo,staged,seg", [(2, 1, 4096), (2, 1, 1024), (2, 1, 512), (2, 1, 2048), (2, 1, 8192),
+                                             (1, 1, 4096), (1, 0, 4096)],
+                         ids=["split", "split-group1k", "split-group512", "split-seg2k", "split-seg8k", "fused-staged",
+                              "fused-l1"])
 @pytest.mark.parametrize("name,spec", cases.CASES, ids=[n for n, _ in cases.CASES])
 def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged, seg):
     z, meta = golden
@@ -76,11 +77,12 @@ def test_compact_host_api_matches_oracle(ctx, name, spec):
     np.testing.assert_array_equal(seqs, o_seqs)
 
 
-@pytest.mark.parametrize("algo,seg,sweep,pf", [(2, 4096, 0, 4), (2, 1024, 0, 4), (2, 1024, 0, 0), (2, 1024, 0, 8),
-                                                (2, 1024, 1, 4), (2, 1024, 1, 0), (2, 1024, 2, 0), (2, 1024, 3, 0),
-                                                (1, 4096, 0, 4)],
-                         ids=["split", "split-group1k", "sweep-no-prefetch", "sweep-prefetch8", "sweep-ballots",
-                              "sweep-ballots-no-prefetch", "sweep-ahead", "sweep-ahead-ballots", "fused"])
+@pytest.mark.parametrize("algo,seg,sweep,pf", [(2, 4096, 0, 4), (2, 1024, 0, 4), (2, 512, 0, 4), (2, 1024, 0, 0),
+                                                (2, 1024, 0, 8), (2, 1024, 1, 4), (2, 1024, 1, 0), (2, 1024, 2, 0),
+                                                (2, 1024, 3, 0), (1, 4096, 0, 4)],
+                         ids=["split", "split-group1k", "split-group512", "sweep-no-prefetch", "sweep-prefetch8",
+                              "sweep-ballots", "sweep-ballots-no-prefetch", "sweep-ahead", "sweep-ahead-ballots",
+                              "fused"])
 @pytest.mark.parametrize("seed,n,mix", [(1, 16 << 20, (0.4, 0.4, 0.2)), (31, 5 << 20, (0.05, 0.9, 0.05)),
                                         (32, 3 << 20 | 12345, (0.9, 0.05, 0.05)), (33, 2 << 20, (0.0, 0.0, 1.0)),
                                         (34, 2 << 20, (0.0, 1.0, 0.0))])
