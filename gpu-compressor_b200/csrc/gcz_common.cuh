@@ -54,6 +54,13 @@ struct SmemWin {
     __device__ __forceinline__ uint32_t byte(uint32_t q) const {
         return reinterpret_cast<const uint8_t *>(w)[q];
     }
+    // The 8 bytes at q: three aligned words, two funnel shifts.
+    __device__ __forceinline__ void u64(uint32_t q, uint32_t &lo, uint32_t &hi) const {
+        const uint32_t i = q >> 2, sh = (q & 3u) * 8u;
+        const uint32_t w1 = w[i + 1];
+        lo = __funnelshift_r(w[i], w1, sh);
+        hi = __funnelshift_r(w1, w[i + 2], sh);
+    }
 };
 
 // Window read in place from global memory (16-byte aligned start).  Only

@@ -290,9 +290,10 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
             const bool cont = lane > 0 && eq4 && ((eq4_bits >> (lane - 1)) & 1u) && c == c_prev + 1u;
             const uint32_t heads = __ballot_sync(kFull, !cont);
             const uint32_t head = 31u - static_cast<uint32_t>(__clz(heads & (lt | (1u << lane))));
-            // Run heads extend their own match for up to 16 more bytes; a head
-            // still matching after that is finished by the whole warp (128 bytes
-            // per iteration), so one long run does not leave 31 lanes idle.
+            // Run heads compare 8 more bytes (bytes 4-11) with one unaligned
+            // 8-byte read of each side, no loop; a head still matching after
+            // that is finished by the whole warp (128 bytes per iteration), so
+            // one long run does not leave 31 lanes idle.
             uint32_t ext = 0;
             const uint32_t bound = size - q < kLzmaMaxMatch + 31u ? size - q : kLzmaMaxMatch + 31u;
             bool pending = false;
@@ -300,8 +301,14 @@ __global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
                 if (lane == 0 && carry_e > 4u && carry_e < kLzmaMaxMatch && c == carry_c + 1u) {
                     ext = carry_e - 1u;  // the previous step's last match, one byte on
                 } else {
-                    const uint32_t lim1 = bound < 20u ? bound : 20u;
-                    ext = extend_lane(win, c, q, 4u, lim1);
+                    const uint32_t lim1 = bound < 12u ? bound : 12u;  // bound >= 4 (q + 3 < size)
+                    uint32_t ql, qh, cl, ch;
+                    win.u64(q + 4u, ql, qh);
+                    win.u64(c + 4u, cl, ch);
+                    const uint32_t dl = ql ^ cl, dh = qh ^ ch;
+                    const uint32_t fb = dl ? (static_cast<uint32_t>(__ffs(dl)) - 1u) >> 3
+                                           : (dh ? 4u + ((static_cast<uint32_t>(__ffs(dh)) - 1u) >> 3) : 8u);
+                    ext = 4u + fb < lim1 ? 4u + fb : lim1;
                     pending = ext == lim1 && lim1 < bound;
                 }
             }

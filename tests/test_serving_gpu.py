@@ -219,24 +219,33 @@ def _check_alone(ctx, kind, depth, data, res):
 
 def test_every_kind_in_one_batch(ctx):
     """Zstd (lazy and greedy), GPU frames and LZMA2 requests submitted together
-    land in one batch (one slot, one candidate sweep over all their windows)
-    and each gets exactly its result alone."""
+    share a batch (one slot, one candidate sweep over all their windows) and
+    each gets exactly its result alone.  The server has one slot, and a 32 MiB
+    LZMA2 request holds it while the eight are submitted, so they are all
+    pending when it frees up and the worker admits them, oldest first, into
+    one batch (two if the submitting thread was held up)."""
     import gcz
     from gcz import serving
 
-    srv = serving.Server(ctx, hbm_budget=4 * 10**9, max_batch_bytes=32 << 20, max_batch_requests=64)
+    srv = serving.Server(ctx, hbm_budget=1_200_000_000, max_batch_bytes=32 << 20, max_batch_requests=64)
+    assert srv.info()[0] == 1
     rng = np.random.default_rng(5)
     plan = [(serving.ZSTD, 16), (serving.LZMA2, 32), (serving.ZSTD_FRAMES, 16), (serving.ZSTD, 1),
             (serving.LZMA2, 32), (serving.ZSTD, 64), (serving.ZSTD_FRAMES, 64), (serving.ZSTD, 16)]
     sizes = [3 << 20, 65537, 1 << 20, 200000, 5, 2 << 20, 70000, 0]
     datas = [gcz.gen_synthetic(1100 + i, n, 8 << 20, tuple(rng.dirichlet([1, 1, 1]))) for i, n in enumerate(sizes)]
+    blocker = gcz.gen_synthetic(1099, 32 << 20, 8 << 20)
     for rep in range(2):
         before = srv.stats()["batches"]
+        rb = srv.submit(serving.LZMA2, blocker, 32)
         reqs = [srv.submit(k, d, depth) for (k, depth), d in zip(plan, datas)]
         res = [srv.wait(r) for r in reqs]
+        srv.wait(rb)
         for (k, depth), d, x in zip(plan, datas, res):
             _check_alone(ctx, k, depth, d, x)
-        assert srv.stats()["batches"] - before <= 2  # the first may launch alone before the rest arrive
+        # the blocker's batch, then the eight in one (or two) batches: admitted
+        # in submit order, so a batch holds more than one kind
+        assert srv.stats()["batches"] - before <= 3
     st = srv.stats()
     srv.close()
     assert st["status"] == 0
