@@ -283,7 +283,7 @@ def load_tuned(ctx, args):
             src = "gcz/tuned/" + os.path.basename(autotune.tuned_path(ctx.device))
     ctx.set_option("algo", args.algo)
     knobs = {k: ctx.query(k) for k in ("algo", "sweep_warps", "sweep_groups", "sweep_prefetch", "parse_seg", "parse_ctas",
-                                       "lzma_ctas", "slice_windows")}
+                                       "lzma_ctas", "lzma_threads", "slice_windows")}
     knobs["source"] = src
     return knobs
 

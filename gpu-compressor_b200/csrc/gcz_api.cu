@@ -77,6 +77,7 @@ struct gcz_ctx {
     int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0/1 after a read-back (match_any/ballots), 2/3 one block ahead
     int sweep_prefetch = 4;  // candidate sweep's L2 prefetch distance of the input, in 128-byte blocks (0, 4, 8)
     int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM
+    int lzma_threads = 512;  // LZMA2 second-stage threads per CTA (256 or 512)
     // profiling
     bool prof = false;
     std::vector<EventPair> events;
@@ -280,6 +281,7 @@ int lzma_run(gcz_ctx *c, Scratch &sc, const gcz::LzmaLaunch &l, cudaStream_t st)
                                            c->sweep_warps, c->sweep_groups, c->sweep_prefetch));
         gcz::LzmaLaunch lv = l;
         lv.ctas_per_sm = c->lzma_ctas;
+        lv.threads = c->lzma_threads;
         GCZ_CUDA(c, gcz::launch_lzma_verify(lv, cand, st));
         c->all_launches += 2;
     } else {
@@ -465,6 +467,10 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->lzma_ctas = (int)value;
         return GCZ_OK;
     }
+    if (!strcmp(key, "lzma_threads") && (value == 256 || value == 512)) {
+        c->lzma_threads = (int)value;
+        return GCZ_OK;
+    }
     return fail(c, GCZ_EINVAL, "unknown option '%s'", key);
 }
 
@@ -496,7 +502,8 @@ extern "C" int gcz_query(gcz_ctx *c, const char *key, long *value) {
     } knobs[] = {{"staged", c->staged},          {"parse_ctas", c->parse_ctas},
                  {"parse_seg", c->seg_width},    {"sweep_warps", c->sweep_warps},
                  {"sweep_groups", c->sweep_groups}, {"sweep_prefetch", c->sweep_prefetch},
-                 {"lzma_ctas", c->lzma_ctas},    {"slice_windows", (long)c->slice_windows},
+                 {"lzma_ctas", c->lzma_ctas},    {"lzma_threads", c->lzma_threads},
+                 {"slice_windows", (long)c->slice_windows},
                  {"frames_slice_windows", (long)c->frames_slice_windows}};
     for (const auto &kv : knobs)
         if (!strcmp(key, kv.k)) {
@@ -1462,6 +1469,7 @@ int server_launch(gcz_server *sv, ServerSlot &s) {
         l.staged = 1;
         l.wins = dw + l0;
         l.ctas_per_sm = c->lzma_ctas;
+        l.threads = c->lzma_threads;
         GCZ_CUDA(c, gcz::launch_lzma_verify(l, cand, s.st));
         for (ServerReq *q : s.reqs) {
             if (q->group != kGrpLzma || !q->n) continue;

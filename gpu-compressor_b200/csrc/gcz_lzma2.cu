@@ -198,7 +198,6 @@ __global__ void __launch_bounds__(256) lzma_unpack_kernel(const uint32_t *packed
 // (its head) extends, up to min(size-q, 273+31) bytes, and the other lanes of
 // the run derive min(273, E_head - (q - head)) from it -- the same value the
 // reference's per-position loop computes with its 273 cap.
-constexpr uint32_t kL2Threads = 256;
 constexpr uint32_t kL2Pre = 64;
 constexpr uint32_t kL2DataBytes = kL2Pre + kMaxWindow + 64;
 
@@ -225,7 +224,10 @@ struct L2Args {
     const WinDesc *wins;
 };
 
-__global__ void __launch_bounds__(kL2Threads) lzma_verify_kernel(L2Args a) {
+// kL2Threads (256 or 512) is a schedule knob: the window's steps are split
+// into kL2Threads / 32 contiguous ranges, one per warp.
+template <uint32_t kL2Threads>
+__global__ void __launch_bounds__(kL2Threads, 3) lzma_verify_kernel(L2Args a) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     L2Smem &S = *reinterpret_cast<L2Smem *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -419,6 +421,20 @@ cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t wind
     return cudaGetLastError();
 }
 
+namespace {
+template <uint32_t kThreads>
+cudaError_t launch_verify_variant(const L2Args &a, const LzmaLaunch &l, cudaStream_t st) {
+    const uint32_t smem = sizeof(L2Smem);
+    static SmemOnce smem_set{0};
+    cudaError_t e = set_smem_once(lzma_verify_kernel<kThreads>, smem, smem_set);
+    if (e != cudaSuccess) return e;
+    int grid = l.num_sms * (l.ctas_per_sm > 0 ? l.ctas_per_sm : 3);
+    if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
+    lzma_verify_kernel<kThreads><<<grid, kThreads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaStream_t st) {
     if (l.num_windows == 0) return cudaSuccess;
     L2Args a{};
@@ -435,14 +451,7 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     a.ref_counts = l.ref_counts;
     a.status = l.status;
     a.wins = l.wins;
-    const uint32_t smem = sizeof(L2Smem);
-    static SmemOnce smem_set_3{0};
-    cudaError_t e = set_smem_once(lzma_verify_kernel, smem, smem_set_3);
-    if (e != cudaSuccess) return e;
-    int grid = l.num_sms * (l.ctas_per_sm > 0 ? l.ctas_per_sm : 3);
-    if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    lzma_verify_kernel<<<grid, kL2Threads, smem, st>>>(a);
-    return cudaGetLastError();
+    return l.threads == 256 ? launch_verify_variant<256>(a, l, st) : launch_verify_variant<512>(a, l, st);
 }
 
 }  // namespace gcz
