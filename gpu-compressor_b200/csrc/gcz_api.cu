@@ -77,7 +77,7 @@ struct gcz_ctx {
     int sweep_groups = 0;  // candidate sweep's equal-hash grouping: 0/1 after a read-back (match_any/ballots), 2/3 one block ahead
     int sweep_prefetch = 4;  // candidate sweep's L2 prefetch distance of the input, in 128-byte blocks (0, 4, 8)
     int lzma_ctas = 3;     // LZMA2 second-stage CTAs per SM
-    int lzma_threads = 512;  // LZMA2 second-stage threads per CTA (256 or 512)
+    int lzma_threads = 1024;  // LZMA2 second-stage threads per CTA (256, 512 or 1024)
     // profiling
     bool prof = false;
     std::vector<EventPair> events;
@@ -467,7 +467,7 @@ extern "C" int gcz_set_option(gcz_ctx *c, const char *key, long value) {
         c->lzma_ctas = (int)value;
         return GCZ_OK;
     }
-    if (!strcmp(key, "lzma_threads") && (value == 256 || value == 512)) {
+    if (!strcmp(key, "lzma_threads") && (value == 256 || value == 512 || value == 1024)) {
         c->lzma_threads = (int)value;
         return GCZ_OK;
     }

@@ -47,7 +47,7 @@ struct LzmaLaunch {
     int staged;
     const WinDesc *wins = nullptr;  // optional window table (second stage only)
     int ctas_per_sm = 3;            // second-stage CTAs per SM (schedule only)
-    int threads = 512;              // second-stage threads per CTA, 256 or 512 (schedule only)
+    int threads = 1024;             // second-stage threads per CTA, 256, 512 or 1024 (schedule only)
 };
 
 // Second-stage Zstd parse after the candidate sweep.

@@ -224,10 +224,11 @@ struct L2Args {
     const WinDesc *wins;
 };
 
-// kL2Threads (256 or 512) is a schedule knob: the window's steps are split
-// into kL2Threads / 32 contiguous ranges, one per warp.
+// kL2Threads (256, 512 or 1024) is a schedule knob: the window's steps are
+// split into kL2Threads / 32 contiguous ranges, one per warp.  Three CTAs
+// share an SM (two of 1024 threads).
 template <uint32_t kL2Threads>
-__global__ void __launch_bounds__(kL2Threads, 3) lzma_verify_kernel(L2Args a) {
+__global__ void __launch_bounds__(kL2Threads, kL2Threads == 1024 ? 2 : 3) lzma_verify_kernel(L2Args a) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     L2Smem &S = *reinterpret_cast<L2Smem *>(smem_raw);
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
@@ -428,7 +429,9 @@ cudaError_t launch_verify_variant(const L2Args &a, const LzmaLaunch &l, cudaStre
     static SmemOnce smem_set{0};
     cudaError_t e = set_smem_once(lzma_verify_kernel<kThreads>, smem, smem_set);
     if (e != cudaSuccess) return e;
-    int grid = l.num_sms * (l.ctas_per_sm > 0 ? l.ctas_per_sm : 3);
+    // no more CTAs than fit on the SMs at once, so that no CTA waits for a second wave
+    const int fit = kThreads == 1024 ? 2 : 3;
+    int grid = l.num_sms * (l.ctas_per_sm > 0 && l.ctas_per_sm < fit ? l.ctas_per_sm : fit);
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
     lzma_verify_kernel<kThreads><<<grid, kThreads, smem, st>>>(a);
     return cudaGetLastError();
@@ -451,7 +454,9 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     a.ref_counts = l.ref_counts;
     a.status = l.status;
     a.wins = l.wins;
-    return l.threads == 256 ? launch_verify_variant<256>(a, l, st) : launch_verify_variant<512>(a, l, st);
+    if (l.threads == 256) return launch_verify_variant<256>(a, l, st);
+    if (l.threads == 512) return launch_verify_variant<512>(a, l, st);
+    return launch_verify_variant<1024>(a, l, st);
 }
 
 }  // namespace gcz

@@ -16,7 +16,7 @@ scheduled:
                         or 512 bytes per 4-lane group (128 segments)
          "parse_ctas"   second-stage CTAs per SM
   LZMA2  "lzma_ctas"    second-stage CTAs per SM (the sweep is shared)
-         "lzma_threads" second-stage threads per CTA (256 or 512)
+         "lzma_threads" second-stage threads per CTA (256, 512 or 1024)
   host   "slice_windows" windows per slice of the host-buffer pipelines
 
 tune_zstd() and tune_lzma2() time every candidate on a sample of the caller's
@@ -46,7 +46,8 @@ ZSTD_CANDIDATES = [
     for seg, ctas_list in ((4096, (3, 2)), (1024, (3, 2)), (512, (3, 2)), (8192, (3, 2)), (2048, (1,)))
     for ctas in ctas_list
 ]
-LZMA_CANDIDATES = [{"lzma_ctas": c, "lzma_threads": t} for t in (512, 256) for c in (3, 2, 1)]
+LZMA_CANDIDATES = [{"lzma_ctas": c, "lzma_threads": t} for t in (512, 256) for c in (3, 2, 1)] + [
+    {"lzma_ctas": c, "lzma_threads": 1024} for c in (2, 1)]
 SLICE_CANDIDATES = [256, 512, 1024, 2048]
 
 

@@ -85,8 +85,9 @@ const char *gcz_version(void);
  * "sweep_prefetch" = how many 128-byte blocks ahead of itself the read-back
  * sweep (groups 0, 1) prefetches its input into L2: 0, 4 (default) or 8;
  * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
- * default 3); "lzma_threads" = LZMA2 second-stage threads per CTA (256 or
- * 512, default 512); "slice_windows" = windows per slice of the host-buffer
+ * default 3, at most 2 with 1024 threads); "lzma_threads" = LZMA2
+ * second-stage threads per CTA (256, 512 or 1024, default 1024);
+ * "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 512 = 32 MiB; four slots, three slices in flight;
  * slices ramp up from a quarter of it and back down at the end);
  * "frames_slice_windows" =

@@ -99,7 +99,7 @@ def test_zstd_batch_replays_in_cuda_graph(ctx):
 
 def _defaults(ctx):
     for k, v in (("algo", 2), ("parse_ctas", 3), ("staged", 1), ("parse_seg", 1024), ("sweep_warps", 7), ("sweep_groups", 0),
-                 ("sweep_prefetch", 4), ("lzma_ctas", 3), ("lzma_threads", 512),
+                 ("sweep_prefetch", 4), ("lzma_ctas", 3), ("lzma_threads", 1024),
                  ("slice_windows", 512)):
         ctx.set_option(k, v)
 

@@ -29,19 +29,22 @@ def run_ref_layout(ctx, data, window, max_matches, depth):
             c.cpu().numpy().view(np.uint32)[:B * window])
 
 
-@pytest.mark.parametrize("algo,staged", [(2, 1), (1, 1), (1, 0)], ids=["split", "fused-staged", "fused-l1"])
+@pytest.mark.parametrize("algo,staged,threads", [(2, 1, 1024), (2, 1, 512), (2, 1, 256), (1, 1, 1024), (1, 0, 1024)],
+                         ids=["split", "split-512", "split-256", "fused-staged", "fused-l1"])
 @pytest.mark.parametrize("name,spec", cases.CASES, ids=[n for n, _ in cases.CASES])
-def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged):
+def test_ref_layout_matches_reference_golden(ctx, golden, name, spec, algo, staged, threads):
     z, meta = golden
     data = cases.build(spec)
     n = data.size
     ctx.set_option("algo", algo)
     ctx.set_option("staged", staged)
+    ctx.set_option("lzma_threads", threads)
     try:
         m, c = run_ref_layout(ctx, data, spec["window"], spec["lmax"], spec["ldepth"])
     finally:
         ctx.set_option("algo", 2)
         ctx.set_option("staged", 1)
+        ctx.set_option("lzma_threads", 1024)
     assert int(c.max(initial=0)) <= 1
     assert not np.any(c[n:])
     assert not np.any(m[:, 1:, :])
