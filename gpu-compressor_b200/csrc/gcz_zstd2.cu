@@ -36,6 +36,8 @@
 //    max_seqs exactly like the reference's `num_seqs < max_sequences_per_chunk`
 //    test (:309): the capped parse emits the first max_seqs matches of the
 //    uncapped one and nothing after them.
+// In the 8- and 4-lane group layouts, once only one group of a warp is still
+// continuing, the whole warp finishes that continuation with warp-wide steps.
 // If a continuation does not meet a later list within kContCap matches the
 // CTA falls back to an exact warp-wide parse of the whole window.
 #include <type_traits>
@@ -828,7 +830,72 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
             uint2 *cl = lst + kSpecCap;
             for (;;) {
                 const bool run = crun && s.p + 3u < size;
-                if (!__any_sync(kFull, run)) break;
+                const uint32_t runners = __ballot_sync(kFull, run && gl == 0u);
+                if (!runners) break;
+                if ((runners & (runners - 1u)) == 0u) {
+                    // Only one group of the warp still runs (the slow tail of the
+                    // phase): the whole warp takes over its parse with warp-wide
+                    // steps (up to 128 positions scanned, 128 bytes extended per
+                    // iteration), same meeting test, then the loop ends.
+                    const uint32_t L = static_cast<uint32_t>(__ffs(runners)) - 1u;
+                    PState ws{__shfl_sync(kFull, s.p, L), __shfl_sync(kFull, s.r0, L), __shfl_sync(kFull, s.r1, L),
+                              __shfl_sync(kFull, s.r2, L)};
+                    const uint32_t wsg = __shfl_sync(kFull, sg, L);
+                    uint32_t wt = __shfl_sync(kFull, t, L), wj = __shfl_sync(kFull, j, L),
+                             wcn = __shfl_sync(kFull, cn, L);
+                    uint2 *wcl = seg + wsg * kLaneCap + kSpecCap;
+                    CandBuf wcb{cand, size, 0u, 0u, 0u, 0u};
+                    wcb.init(ws.p);
+                    while (ws.p + 3u < size) {
+                        Match m;
+                        if (!warp_step(win, S.bm, wcb, size, lazy, ws, m)) continue;
+                        const uint32_t tw = m.start / kSegW;  // segment that holds this match start
+                        if (tw != wt) {
+                            wt = tw;
+                            wj = 0;
+                        }
+                        const uint32_t tcount = S.spec_count[wt];
+                        const uint2 *tl = seg + wt * kLaneCap;
+                        // first entry of wt's list with start >= m.start, 32 per step
+                        for (;;) {
+                            const uint32_t idx = wj + lane;
+                            const bool ge = idx >= tcount || (tl[idx].x & 0xFFFFu) >= m.start;
+                            const uint32_t b = __ballot_sync(kFull, ge);
+                            if (b) {
+                                wj += static_cast<uint32_t>(__ffs(b)) - 1u;
+                                break;
+                            }
+                            wj += 32u;
+                        }
+                        bool met = false;
+                        if (wj < tcount) {
+                            const uint2 e = tl[wj];
+                            if (e.x == pack_entry(m).x && e.y == m.off) {
+                                uint32_t e0, e1, e2;
+                                reps_after(tl, wj, e0, e1, e2);
+                                met = e0 == ws.r0 && e1 == ws.r1 && e2 == ws.r2;
+                            }
+                        }
+                        if (met) {
+                            if (lane == 0) {
+                                S.sync_warp[wsg] = wt;
+                                S.sync_idx[wsg] = wj;
+                            }
+                            break;
+                        }
+                        if (wcn == kContCap) {
+                            if (lane == 0) atomicOr(&S.flags, 1u);  // give up: exact fallback below
+                            break;
+                        }
+                        if (lane == 0) wcl[wcn] = pack_entry(m);
+                        ++wcn;
+                    }
+                    if (lane >= L && lane < L + GL) {
+                        cn = wcn;
+                        crun = false;
+                    }
+                    break;
+                }
                 Match m;
                 const bool ev = group_step<GL>(win, S.bm, cand, size, lazy, run, s, m);
                 uint32_t tcount = 0;
