@@ -51,10 +51,9 @@ __device__ __forceinline__ uint32_t same_key_lanes(uint32_t key, bool valid) {
     return valid ? m : (1u << lane_id());
 }
 
-// One 128-position block of a window's sweep: lane l holds word l of the
-// block (w0) and word l of the next block (w1; only lane 0's is used).
-// The block's hashes (independent of the table): step j, lane l is position
-// blk * 128 + 32 j + l.
+// The hashes of one 128-position block (independent of the table): step j,
+// lane l is position blk * 128 + 32 j + l.  Lane l holds word l of the block
+// (w0) and word l of the next block (w1; only lane 0's is used).
 __device__ __forceinline__ void block_hashes(uint32_t blk, uint32_t size, uint32_t w0, uint32_t w1, uint32_t *h,
                                              bool *v) {
     const uint32_t lane = lane_id();
@@ -133,6 +132,7 @@ __device__ __forceinline__ void block_table(uint16_t *T, uint16_t *out, uint32_t
     }
 }
 
+// One 128-position block of a window's sweep: hashes, then table work.
 template <bool kBallotGroups>
 __device__ __forceinline__ void sweep_block(uint16_t *T, uint16_t *out, uint32_t blk, uint32_t size, uint32_t w0,
                                             uint32_t w1, uint32_t lt, uint32_t gt) {
@@ -173,22 +173,20 @@ __global__ void __launch_bounds__(32 * kSweepWarpsPerCta) cand_sweep_kernel(Swee
         const uint32_t nwords = (size + 3u) >> 2;
         uint16_t *out = a.cand + start;
         const uint32_t nblk = (size + 127u) >> 7;
-        {
-            // 128-byte blocks: lane l holds word l.  Each block's words are
-            // loaded two blocks ahead of its sweep; with kPf > 0 lane 0 also
-            // prefetches block b + kPf into L2 while block b is swept, so that
-            // those loads hit L2 instead of waiting on DRAM.
-            uint32_t w0 = block_word(src32, nwords, 0), w1 = block_word(src32, nwords, 1);
-            for (uint32_t blk = 0; blk < nblk; ++blk) {
-                if constexpr (kPf > 0) {
-                    const uint32_t pw = (blk + kPf) * 32u;
-                    if (lane == 0 && pw < nwords) asm volatile("prefetch.global.L2 [%0];" ::"l"(src32 + pw));
-                }
-                const uint32_t w2 = block_word(src32, nwords, blk + 2u);
-                sweep_block<kBallotGroups>(T, out, blk, size, w0, w1, lt, gt);
-                w0 = w1;
-                w1 = w2;
+        // 128-byte blocks: lane l holds word l.  Each block's words are loaded
+        // two blocks ahead of its sweep; with kPf > 0 lane 0 also prefetches
+        // block b + kPf into L2 while block b is swept, so that those loads hit
+        // L2 instead of waiting on DRAM.
+        uint32_t w0 = block_word(src32, nwords, 0), w1 = block_word(src32, nwords, 1);
+        for (uint32_t blk = 0; blk < nblk; ++blk) {
+            if constexpr (kPf > 0) {
+                const uint32_t pw = (blk + kPf) * 32u;
+                if (lane == 0 && pw < nwords) asm volatile("prefetch.global.L2 [%0];" ::"l"(src32 + pw));
             }
+            const uint32_t w2 = block_word(src32, nwords, blk + 2u);
+            sweep_block<kBallotGroups>(T, out, blk, size, w0, w1, lt, gt);
+            w0 = w1;
+            w1 = w2;
         }
         __syncwarp();
     }

@@ -84,9 +84,10 @@ const char *gcz_version(void);
  * for every step one block ahead of the table work (2, 3 likewise);
  * "sweep_prefetch" = how many 128-byte blocks ahead of itself the read-back
  * sweep (groups 0, 1) prefetches its input into L2: 0, 4 (default) or 8;
- * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8,
- * default 3, at most 2 with 1024 threads); "lzma_threads" = LZMA2
- * second-stage threads per CTA (256, 512 or 1024, default 1024);
+ * "lzma_ctas" = LZMA2 second-stage CTAs per SM (1-8, default 3; values above
+ * what fits on an SM -- 3, or 2 with 1024 threads -- run as that many);
+ * "lzma_threads" = LZMA2 second-stage threads per CTA (256, 512 or 1024,
+ * default 1024);
  * "slice_windows" = windows per slice of the host-buffer
  * pipelines (default 512 = 32 MiB; four slots, three slices in flight;
  * slices ramp up from a quarter of it and back down at the end);
