@@ -956,8 +956,77 @@ __global__ void __launch_bounds__(SegCfg<SegW, GL>::kThreads, SegCfg<SegW, GL>::
         }
 
         if (!(S.flags & 1u)) {
-            // ---- 3. chain walk (one thread), then copy in chain order
-            if (tid == 0) {
+            // ---- 3. chain walk, then copy in chain order.  Nearly always every
+            // continuation meets the next segment's list, so the chain is
+            // segments 0..K in order (K: the first segment with no link): warp
+            // 0 then sets it up at once -- output offsets by a scan of the
+            // segments' contributions, each segment's preceding entry by a max
+            // scan (entry indices grow with the segment).  Otherwise one
+            // thread walks the links.
+            bool chained = false;
+            if (warp == 0 && lim_pos > 0) {
+                constexpr uint32_t kPer = (kSegs + 31u) / 32u;  // segments per lane, contiguous
+                uint32_t kf = kSegs;
+                bool gap = false;
+#pragma unroll
+                for (uint32_t u = 0; u < kPer; ++u) {
+                    const uint32_t i = lane * kPer + u;
+                    if (i < kSegs && S.sync_warp[i] == kNoWarp && i < kf) kf = i;
+                }
+                const uint32_t K = __reduce_min_sync(kFull, kf);  // segment 0 always parses, so K < kSegs
+#pragma unroll
+                for (uint32_t u = 0; u < kPer; ++u) {
+                    const uint32_t i = lane * kPer + u;
+                    if (i < K && S.sync_warp[i] != i + 1u) gap = true;
+                }
+                chained = !__any_sync(kFull, gap);
+                if (chained) {
+                    uint32_t con[kPer], lst1[kPer], sum = 0, lmax = 0;
+#pragma unroll
+                    for (uint32_t u = 0; u < kPer; ++u) {
+                        const uint32_t i = lane * kPer + u;
+                        con[u] = 0;
+                        lst1[u] = 0;
+                        if (i <= K) {
+                            const uint32_t from = i ? static_cast<uint32_t>(S.sync_idx[i - 1u]) : 0u;
+                            const uint32_t ns = S.spec_count[i], nc = S.cont_count[i];
+                            con[u] = ns - from + nc;
+                            if (con[u]) lst1[u] = 1u + i * kLaneCap + (nc ? kSpecCap + nc - 1u : ns - 1u);
+                        }
+                        sum += con[u];
+                        lmax = lst1[u] > lmax ? lst1[u] : lmax;
+                    }
+                    // exclusive scans over the lanes: sum of contributions, max of last entries (+1)
+                    uint32_t incl = sum, mx = lmax;
+#pragma unroll
+                    for (uint32_t d = 1; d < 32u; d <<= 1) {
+                        const uint32_t o = __shfl_up_sync(kFull, incl, d), om = __shfl_up_sync(kFull, mx, d);
+                        if (lane >= d) {
+                            incl += o;
+                            mx = om > mx ? om : mx;
+                        }
+                    }
+                    uint32_t acc = incl - sum, last1 = __shfl_up_sync(kFull, mx, 1);
+                    if (lane == 0) last1 = 0;
+#pragma unroll
+                    for (uint32_t u = 0; u < kPer; ++u) {
+                        const uint32_t i = lane * kPer + u;
+                        if (i >= kSegs) continue;
+                        const bool on = i <= K;
+                        S.on_chain[i] = on ? 1u : 0u;
+                        if (on) {
+                            S.chain_from[i] = i ? S.sync_idx[i - 1u] : 0u;
+                            S.out_off[i] = acc;
+                            S.prev_last[i] = last1 ? last1 - 1u : kNoEntry;
+                        }
+                        acc += con[u];
+                        last1 = lst1[u] > last1 ? lst1[u] : last1;
+                    }
+                    if (lane == 31u) S.total = incl;
+                }
+            }
+            chained = __syncthreads_or(chained);
+            if (tid == 0 && !chained) {
                 for (uint32_t i = 0; i < kSegs; ++i) S.on_chain[i] = 0;
                 uint32_t cur = 0, from = 0, acc = 0, last = kNoEntry;
                 if (lim_pos > 0) {
