@@ -226,8 +226,10 @@ struct L2Args {
 
 // kL2Threads (256, 512 or 1024) is a schedule knob: the window's steps are
 // split into kL2Threads / 32 contiguous ranges, one per warp.  Three CTAs
-// share an SM (two of 1024 threads).
-template <uint32_t kL2Threads>
+// share an SM (two of 1024 threads).  kRefOut: the reference layout's
+// per-position counts and match slots are written too (the parity entry
+// points); without it the step loop carries no code for them.
+template <uint32_t kL2Threads, bool kRefOut>
 __global__ void __launch_bounds__(kL2Threads, kL2Threads == 1024 ? 2 : 3) lzma_verify_kernel(L2Args a) {
     extern __shared__ __align__(128) uint8_t smem_raw[];
     L2Smem &S = *reinterpret_cast<L2Smem *>(smem_raw);
@@ -259,8 +261,8 @@ __global__ void __launch_bounds__(kL2Threads, kL2Threads == 1024 ? 2 : 3) lzma_v
         if (S.flags) return;
         const uint16_t *cand = a.cand + start;
         uint32_t *packed = a.packed ? a.packed + start : nullptr;
-        uint32_t *rc = a.ref_counts ? a.ref_counts + start : nullptr;
-        uint32_t *rm = a.ref_matches ? a.ref_matches + start * a.max_matches * 2u : nullptr;
+        uint32_t *rc = kRefOut && a.ref_counts ? a.ref_counts + start : nullptr;
+        uint32_t *rm = kRefOut && a.ref_matches ? a.ref_matches + start * a.max_matches * 2u : nullptr;
         uint32_t any = 0;
         const uint32_t nsteps = (size + 31u) >> 5;
         // Each warp takes a contiguous range of steps, so a run of matches
@@ -364,8 +366,8 @@ __global__ void __launch_bounds__(kL2Threads, kL2Threads == 1024 ? 2 : 3) lzma_v
             }
             if (inwin) {
                 if (packed) packed[q] = len ? ((len << 16) | dist) : 0u;
-                if (rc) rc[q] = len ? 1u : 0u;
-                if (rm && len) {
+                if (kRefOut && rc) rc[q] = len ? 1u : 0u;
+                if (kRefOut && rm && len) {
                     uint32_t *slot = rm + static_cast<uint64_t>(q) * a.max_matches * 2u;
                     slot[0] = dist;
                     slot[1] = len;
@@ -373,7 +375,7 @@ __global__ void __launch_bounds__(kL2Threads, kL2Threads == 1024 ? 2 : 3) lzma_v
             }
             any |= len;
         }
-        if (rc)
+        if (kRefOut && rc)
             for (uint32_t q = size + tid; q < a.window; q += kL2Threads) rc[q] = 0u;  // :188-190
         if (__any_sync(kFull, any != 0) && lane == 0) S.any = 1u;
         __syncthreads();
@@ -423,17 +425,17 @@ cudaError_t launch_lzma_unpack(const uint32_t *packed, uint64_t n, uint32_t wind
 }
 
 namespace {
-template <uint32_t kThreads>
+template <uint32_t kThreads, bool kRefOut>
 cudaError_t launch_verify_variant(const L2Args &a, const LzmaLaunch &l, cudaStream_t st) {
     const uint32_t smem = sizeof(L2Smem);
     static SmemOnce smem_set{0};
-    cudaError_t e = set_smem_once(lzma_verify_kernel<kThreads>, smem, smem_set);
+    cudaError_t e = set_smem_once(lzma_verify_kernel<kThreads, kRefOut>, smem, smem_set);
     if (e != cudaSuccess) return e;
     // no more CTAs than fit on the SMs at once, so that no CTA waits for a second wave
     const int fit = kThreads == 1024 ? 2 : 3;
     int grid = l.num_sms * (l.ctas_per_sm > 0 && l.ctas_per_sm < fit ? l.ctas_per_sm : fit);
     if (static_cast<uint32_t>(grid) > l.num_windows) grid = static_cast<int>(l.num_windows);
-    lzma_verify_kernel<kThreads><<<grid, kThreads, smem, st>>>(a);
+    lzma_verify_kernel<kThreads, kRefOut><<<grid, kThreads, smem, st>>>(a);
     return cudaGetLastError();
 }
 }  // namespace
@@ -454,9 +456,14 @@ cudaError_t launch_lzma_verify(const LzmaLaunch &l, const uint16_t *cand, cudaSt
     a.ref_counts = l.ref_counts;
     a.status = l.status;
     a.wins = l.wins;
-    if (l.threads == 256) return launch_verify_variant<256>(a, l, st);
-    if (l.threads == 512) return launch_verify_variant<512>(a, l, st);
-    return launch_verify_variant<1024>(a, l, st);
+    if (a.ref_counts || a.ref_matches) {
+        if (l.threads == 256) return launch_verify_variant<256, true>(a, l, st);
+        if (l.threads == 512) return launch_verify_variant<512, true>(a, l, st);
+        return launch_verify_variant<1024, true>(a, l, st);
+    }
+    if (l.threads == 256) return launch_verify_variant<256, false>(a, l, st);
+    if (l.threads == 512) return launch_verify_variant<512, false>(a, l, st);
+    return launch_verify_variant<1024, false>(a, l, st);
 }
 
 }  // namespace gcz
